@@ -1,0 +1,267 @@
+/* ispm_b200.h -- C ABI of the B200-native ispm-sparse-lib hot path.
+ *
+ * Plain pointers and sizes only: no C++, CUDA or torch types cross this
+ * boundary (streams are passed as void *, i.e. a cudaStream_t; NULL is the
+ * legacy default stream the reference runs on).  Every entry point returns
+ * an ISPM_* status code instead of aborting the process the way the
+ * reference's CUDA_CHECK does (util/cuda/check.h:8-15); ispm_last_error()
+ * gives the message of the calling thread's last failure.
+ *
+ * Each declaration names the reference interface it replaces
+ * (path:line within the reference project).
+ *
+ * Pointer conventions: "host" pointers are ordinary process memory, "device"
+ * pointers are global memory of the current CUDA device (the reference's
+ * devmem<T> / vector<T, device_memory_space_tag>).
+ */
+#ifndef ISPM_B200_H
+#define ISPM_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define ISPM_OK 0
+#define ISPM_ERR_INVALID 1        /* bad argument or unsupported combination */
+#define ISPM_ERR_CUDA 2           /* a CUDA runtime call failed */
+#define ISPM_ERR_NOMEM 3          /* host or device allocation failed */
+#define ISPM_ERR_ARCH 4           /* device is not sm_100 */
+#define ISPM_ERR_BREAKDOWN 5      /* solver breakdown (zero / negative curvature) */
+#define ISPM_ERR_NOT_CONVERGED 6  /* iteration limit reached before the target */
+#define ISPM_ERR_TIMEOUT 7        /* a bounded device-side wait ran out */
+#define ISPM_ERR_TOO_LARGE 8      /* size beyond a documented maximum */
+
+/* element / vector types */
+#define ISPM_F32 0
+#define ISPM_F64 1
+
+const char *ispm_error_string(int status);
+/* Message of the calling thread's most recent failing call ("" if none). */
+const char *ispm_last_error(void);
+/* Library version string. */
+const char *ispm_version(void);
+
+/* ---- device initialisation (util/cuda/initialize.h:4-10,
+ *      util/cuda/initialize.cu:17-42) --------------------------------------
+ * Checks that the current device is compute capability 10.0 (sm_100) --
+ * ISPM_ERR_ARCH otherwise, where the reference aborts -- and sets
+ * cudaDeviceMapHost like the reference does.  The reference's 8-byte shared
+ * memory bank request has no effect on sm_100 and is not made. */
+int ispm_initialize(void);
+/* "dddd:bb:dd (name)" of the current device into buf (at most len bytes). */
+int ispm_get_device_string(char *buf, int len);
+
+/* ---- sliced-ELLPACK matrices (formats/formats.h:39-102) ---------------- */
+
+/* Plain view of one sliced-ELL matrix: the fields of slell_matrix<E, space>
+ * (formats/formats.h:44-55) plus the lengths of its three arrays and the
+ * tallest slice.  The arrays are host or device memory depending on where the
+ * view came from. */
+typedef struct {
+  int n_rows;          /* rows after padding to a multiple of 512 */
+  int n_cols;
+  int n_nz;            /* non-zeros of the source CSR */
+  unsigned slice_height;
+  unsigned n_slices;
+  unsigned hblock;     /* 1, 2 or 4 */
+  int var_height;
+  int diags;
+  int elm_dtype;       /* ISPM_F32 / ISPM_F64 */
+  unsigned min_slice_height; /* shortest / tallest slice (equal unless var_height) */
+  unsigned max_slice_height;
+  long long n_slice_ptr;
+  long long n_cols_arr;
+  long long n_elms;
+  const unsigned *slice_ptr;
+  const unsigned *cols;
+  const void *elms;
+} ispm_slell_view;
+
+/* slell_params (formats/formats.h:39-42) */
+typedef struct {
+  unsigned S, H, V, D; /* slice height, hblock width, var height, diagonals */
+} ispm_slell_params;
+
+typedef struct ispm_slell ispm_slell;   /* host matrix  (host_memory_space_tag) */
+typedef struct ispm_dslell ispm_dslell; /* device matrix (device_memory_space_tag) */
+
+/* csr_to_slell (formats/conversion.h:338-414).  Converts an n_rows x n_cols
+ * CSR (row_ptr[n_rows + 1], cols[nnz], elms[nnz] of elm_dtype, host memory)
+ * into a host sliced-ELL matrix.  Result layout is bit-identical to the
+ * reference's.  The reference pads the caller's CSR to a multiple of 512 rows
+ * in place (conversion.h:343); this entry point leaves the caller's arrays
+ * untouched and reports the padded row count in the result's n_rows.
+ * A fixed slice height must divide the padded row count (the reference reads
+ * past the CSR otherwise): ISPM_ERR_INVALID. */
+int ispm_csr_to_slell(int elm_dtype, int n_rows, int n_cols, const int *row_ptr,
+                      const int *cols, const void *elms, int slice_height, int hblock,
+                      int var_height, int use_diags, int min_height, ispm_slell **out);
+
+/* csr_to_slell_guess_format (formats/conversion.h:416-492): picks slice
+ * height, hblock width, variable height and diagonal extraction from the first
+ * examine_ratio percent of rows, then converts. Rows past n_rows read as empty
+ * (the reference reads them unpadded for matrices under ~3,200 rows). */
+int ispm_csr_to_slell_guess_format(int elm_dtype, int n_rows, int n_cols, const int *row_ptr,
+                                   const int *cols, const void *elms, int examine_ratio,
+                                   int min_height, ispm_slell **out);
+
+/* View of a host matrix's arrays; valid until the matrix is freed. */
+int ispm_slell_get_view(const ispm_slell *m, ispm_slell_view *view);
+/* Mutable host element array (the public slell_matrix::elms member the
+ * reference's callers edit before update_device_matrix_coefs). */
+void *ispm_slell_elms(ispm_slell *m);
+/* slell_matrix::spmv_bytes (formats/formats.h:72-78) with the vector element
+ * size honoured (the reference always counts 4 bytes: sizeof(vec_elt_size)). */
+unsigned long long ispm_slell_spmv_bytes(const ispm_slell *m, int effective, int vec_elt_size);
+void ispm_slell_free(ispm_slell *m);
+
+/* slell_matrix<E, device> copy constructor (formats/formats.h:56-66): upload
+ * a host matrix to the current device. */
+int ispm_dslell_upload(const ispm_slell *h, ispm_dslell **out);
+/* Re-upload only the element values of a matrix with unchanged structure
+ * (plan/plan.h:39-42, implemented as the element-only H2D copy it means). */
+int ispm_dslell_update_elms(ispm_dslell *d, const ispm_slell *h);
+/* View of a device matrix's arrays (device pointers). */
+int ispm_dslell_get_view(const ispm_dslell *d, ispm_slell_view *view);
+void ispm_dslell_free(ispm_dslell *d);
+
+/* ---- SpMV launch (cuda/spmv/kernel-iface.h:6-74, cuda/spmv/dispatch.h) -- */
+
+/* spmv_launch_params (kernel-iface.h:6-17).  N = threads cooperating on one
+ * slice, S = slice height the launch is specialised for, H = consecutive rows
+ * per thread.  use_tex_* are accepted for source compatibility and ignored:
+ * sm_100 has no texture references; x goes through the read-only data path. */
+typedef struct {
+  unsigned N, S, H;
+  int use_tex_sliceptr;
+  int use_tex_x;
+} ispm_launch_params;
+
+/* SPMV_PARAMS_VALID_P (kernel-iface.h:4): N >= S / H && S >= H. */
+int ispm_launch_params_valid(const ispm_launch_params *p);
+
+/* launch_spmv_kernel<T, E> (kernel-iface.h:20-74): y = A x on `stream`.
+ * x_dtype is T (ISPM_F32 / ISPM_F64), A's elm_dtype is E; (T, E) must be one
+ * of the reference's instantiations (float,float), (double,float),
+ * (double,double).  x holds n_cols values of T, y n_rows (padded) values of T.
+ * Where the reference silently launches nothing for unsupported parameters
+ * (dispatch.h:131,143,166,180,202-203), this returns ISPM_ERR_INVALID.
+ * Supported: N a power of two in [4, 1024]; H in {1, 2, 4}; S the matrix's
+ * slice height (fixed-height matrices) and N * H >= every slice's height. */
+int ispm_launch_spmv(int x_dtype, const ispm_launch_params *p, const ispm_slell_view *m,
+                     const void *x, void *y, void *stream);
+
+/* ---- autotuning plan (plan/plan.h:9-161) -------------------------------- */
+#define ISPM_PLAN_DEFAULT 0
+#define ISPM_PLAN_ESTIMATE 1
+#define ISPM_PLAN_EXHAUSTIVE 2
+#define ISPM_SPMV_NO_TEXTURE_MEMORY 1
+#define ISPM_SPMV_PLAN_NO_DEVICE 2
+
+typedef struct ispm_plan ispm_plan;
+
+/* spmv_plan<T, E>(csr_matrix<E>, kind, flags) (plan/plan.h:64-146).
+ * DEFAULT/ESTIMATE: guessed format, launch parameters from a B200 heuristic.
+ * EXHAUSTIVE: the reference's format grid (S 32..512, V, D, hblock 1/2) widened
+ * with hblock 4, and every launch shape timed with CUDA events (median of
+ * repeats) instead of one timed launch. */
+int ispm_plan_create(int vec_dtype, int elm_dtype, int n_rows, int n_cols, const int *row_ptr,
+                     const int *cols, const void *elms, int kind, unsigned flags,
+                     ispm_plan **out);
+/* spmv_plan::execute_spmv (plan/plan.h:148-161) */
+int ispm_plan_execute(ispm_plan *p, const void *x, void *y, void *stream);
+/* spmv_plan::upload (plan/plan.h:44-49) */
+int ispm_plan_upload(ispm_plan *p);
+/* spmv_plan::update_device_matrix_coefs (plan/plan.h:39-42) */
+int ispm_plan_update_device_matrix_coefs(ispm_plan *p);
+/* spmv_plan::change_host_matrix (plan/plan.h:51-56): re-convert a new CSR
+ * with the plan's stored format parameters (host matrix only). */
+int ispm_plan_change_host_matrix(ispm_plan *p, int n_rows, int n_cols, const int *row_ptr,
+                                 const int *cols, const void *elms);
+int ispm_plan_get_params(const ispm_plan *p, ispm_slell_params *mparams,
+                         ispm_launch_params *params);
+/* The plan's matrices (NULL if absent); owned by the plan. */
+ispm_slell *ispm_plan_host_matrix(ispm_plan *p);
+const ispm_dslell *ispm_plan_device_matrix(const ispm_plan *p);
+/* Best time (seconds) an EXHAUSTIVE plan measured, else 0. */
+double ispm_plan_tuned_seconds(const ispm_plan *p);
+void ispm_plan_free(ispm_plan *p);
+
+/* ---- sblas: BLAS-1 and pipelined-CG fusions (util/cuda/sblas.h:1-56) ----
+ * All vector and scalar pointers are device pointers of dtype T.
+ * Reductions accumulate in FP64 whatever T is (the reference accumulates in
+ * T) and finish inside the same launch (the reference adds a one-block
+ * launch).  They use a per-device scratch area allocated on first use, so
+ * calls that overlap on the GPU (different streams, or threads) race on it,
+ * exactly as the reference's full_launch singleton does. */
+
+/* sblas::copy_indexed (sblas.cu:18-33): dst[k] = src[idx[k]], k < n. */
+int ispm_sblas_copy_indexed(int dtype, void *dst, const void *src, const int *idx, int n,
+                            void *stream);
+/* sblas::add_indexed (sblas.cu:36-51): dst[idx[k]] += src[k].  Uses atomic
+ * adds, so repeated indices all count (the reference races on them). */
+int ispm_sblas_add_indexed(int dtype, void *dst, const void *src, const int *idx, int n,
+                           void *stream);
+/* sblas::dot (sblas.cu:126-153): *s = sum x_i y_i. */
+int ispm_sblas_dot(int dtype, const void *x, const void *y, void *s, int n, void *stream);
+/* sblas::ppcg_update_scalars (sblas.cu:156-174):
+ * beta = gamma / gammaold; alpha = gamma / (delta - beta * gamma / alpha). */
+int ispm_sblas_ppcg_update_scalars(int dtype, void *alpha, void *beta, const void *gamma,
+                                   const void *gammaold, const void *delta, void *stream);
+/* sblas::ppcg_update_vectors (sblas.cu:177-237): z = n + beta z;
+ * q = m + beta q; s = w + beta s; p = u + beta p; u -= alpha q; w -= alpha z;
+ * r -= alpha s; x += alpha p; then *resnorm = sum |r_i|, *gamma = r.u,
+ * *delta = w.u of the updated vectors. */
+int ispm_sblas_ppcg_update_vectors(int dtype, void *resnorm, void *gamma, void *delta,
+                                   const void *alpha, const void *beta, const void *n,
+                                   const void *m, void *p, void *s, void *q, void *z, void *x,
+                                   void *r, void *u, void *w, int n_elts, void *stream);
+
+/* ---- approximate inverse (fastainv/fastainv.h:8-30) --------------------- */
+
+typedef struct ispm_csr ispm_csr; /* host CSR owned by the library */
+typedef void (*ispm_progress_f)(void *);
+
+typedef struct {
+  long long storage_chunks;   /* chunk capacity after the maxneed cap */
+  long long chunks_used;
+  long long truncated_rows;   /* row updates cut short by exhausted storage */
+  long long breakdowns;       /* pivots D_jj == 0 (row scale set to 0) */
+} ispm_fastainv_stats;
+
+/* fastainv_sym<double, out_real> (fastainv/fastainv.cpp:395-566).  A is an
+ * n x n symmetric CSR in FP64 (host).  Produces Ainv1 (= G) and Ainv2 (= G^T
+ * with unsigned scale), so that Ainv2 * Ainv1 ~ A^-1, bit-identical to the
+ * reference for out_dtype FP64 (double,double) and FP32 (double,float).
+ * progress(v) is called once per row as in the reference (may be NULL).
+ * Returns ISPM_ERR_INVALID for n <= 0 (the reference returns false).
+ * stats may be NULL; storage exhaustion truncates rows exactly as the
+ * reference does (fastainv.cpp:74-78) and is counted in stats. */
+int ispm_fastainv_sym(int out_dtype, int n, const int *row_ptr, const int *cols,
+                      const double *elms, ispm_progress_f progress, void *v,
+                      long long max_elts, double droptol, ispm_csr **ainv1, ispm_csr **ainv2,
+                      ispm_fastainv_stats *stats);
+int ispm_csr_get_info(const ispm_csr *m, int *n_rows, int *n_cols, int *n_nz, int *dtype);
+/* Host views of the CSR arrays; valid until ispm_csr_free. */
+int ispm_csr_get_arrays(const ispm_csr *m, const int **row_ptr, const int **cols,
+                        const void **elms);
+void ispm_csr_free(ispm_csr *m);
+
+/* ---- drop-tolerance tuner (fastainv/droptol-tuning.h:4-103) ------------ */
+typedef struct ispm_droptol_tuner ispm_droptol_tuner;
+ispm_droptol_tuner *ispm_droptol_tuner_create(double lo, double hi);
+double ispm_droptol_tuner_get_droptol(const ispm_droptol_tuner *t);
+double ispm_droptol_tuner_get_best_droptol(const ispm_droptol_tuner *t);
+void ispm_droptol_tuner_note_time(ispm_droptol_tuner *t, double time);
+void ispm_droptol_tuner_restart(ispm_droptol_tuner *t);
+void ispm_droptol_tuner_reset_phase(ispm_droptol_tuner *t);
+int ispm_droptol_tuner_iterations(const ispm_droptol_tuner *t);
+void ispm_droptol_tuner_free(ispm_droptol_tuner *t);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,84 @@
+// CUDA helpers shared by the library's .cu files (sm_100a only).
+#ifndef ISPM_CUDA_UTIL_CUH
+#define ISPM_CUDA_UTIL_CUH
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "ispm_internal.h"
+
+#define ISPM_CUDA_TRY(call)                                                                 \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      return ::ispm::fail(ISPM_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_),   \
+                          __FILE__, __LINE__);                                              \
+  } while (0)
+
+namespace ispm {
+
+inline bool aligned(const void *p, size_t a) { return ((uintptr_t)p & (a - 1)) == 0; }
+inline bool is_pow2(unsigned v) { return v && !(v & (v - 1)); }
+inline int ilog2(unsigned v) { return 31 - __builtin_clz(v); }
+
+int device_sm_count();
+
+// ---- device-side load helpers --------------------------------------------
+
+// Streaming (evict-first) loads for matrix data read exactly once per SpMV.
+template <int N, class V> struct Vec {
+  V v[N];
+};
+
+template <int N, class V> __device__ __forceinline__ Vec<N, V> ld_stream(const V *p)
+{
+  Vec<N, V> r;
+  constexpr int bytes = N * (int)sizeof(V);
+  if constexpr (bytes == 4) {
+    if constexpr (sizeof(V) == 4 && N == 1) {
+      *reinterpret_cast<unsigned *>(&r.v[0]) = __ldcs(reinterpret_cast<const unsigned *>(p));
+    }
+  } else if constexpr (bytes == 8) {
+    uint2 t = __ldcs(reinterpret_cast<const uint2 *>(p));
+    *reinterpret_cast<uint2 *>(r.v) = t;
+  } else if constexpr (bytes == 16) {
+    uint4 t = __ldcs(reinterpret_cast<const uint4 *>(p));
+    *reinterpret_cast<uint4 *>(r.v) = t;
+  } else {
+    static_assert(bytes == 32, "vector width");
+    const uint4 *q = reinterpret_cast<const uint4 *>(p);
+    uint4 a = __ldcs(q), b = __ldcs(q + 1);
+    reinterpret_cast<uint4 *>(r.v)[0] = a;
+    reinterpret_cast<uint4 *>(r.v)[1] = b;
+  }
+  return r;
+}
+
+// Read-only-path load for the gathered vector x (kept in L1/L2).
+template <class T> __device__ __forceinline__ T ld_x(const T *x, unsigned i) { return __ldg(x + i); }
+
+template <class T> __device__ __forceinline__ T ld_x_guard(const T *x, unsigned i, unsigned n)
+{
+  return i < n ? __ldg(x + i) : T(0);
+}
+
+template <int N, class T> __device__ __forceinline__ void st_vec(T *p, const T (&v)[N])
+{
+  constexpr int bytes = N * (int)sizeof(T);
+  if constexpr (bytes == 4 || bytes == 8 || bytes == 16) {
+    if constexpr (bytes == 4)
+      *reinterpret_cast<unsigned *>(p) = *reinterpret_cast<const unsigned *>(v);
+    else if constexpr (bytes == 8)
+      *reinterpret_cast<uint2 *>(p) = *reinterpret_cast<const uint2 *>(v);
+    else
+      *reinterpret_cast<uint4 *>(p) = *reinterpret_cast<const uint4 *>(v);
+  } else {
+    reinterpret_cast<uint4 *>(p)[0] = reinterpret_cast<const uint4 *>(v)[0];
+    reinterpret_cast<uint4 *>(p)[1] = reinterpret_cast<const uint4 *>(v)[1];
+  }
+}
+
+}  // namespace ispm
+
+#endif

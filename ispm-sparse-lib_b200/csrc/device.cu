@@ -1,0 +1,212 @@
+// Device initialisation and device-resident sliced-ELL matrices.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "cuda_util.cuh"
+#include "spmv_launch.h"
+
+namespace ispm {
+
+int device_sm_count()
+{
+  static std::mutex mu;
+  static int cached[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+    return 148;
+  std::lock_guard<std::mutex> g(mu);
+  if (!cached[dev]) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
+      v = 148;
+    cached[dev] = v;
+  }
+  return cached[dev];
+}
+
+static size_t elm_size(int dtype) { return dtype == ISPM_F32 ? 4 : 8; }
+
+void DeviceSlell::release()
+{
+  if (slice_ptr)
+    cudaFree(slice_ptr);
+  if (cols)
+    cudaFree(cols);
+  if (elms)
+    cudaFree(elms);
+  slice_ptr = nullptr;
+  cols = nullptr;
+  elms = nullptr;
+}
+
+int DeviceSlell::upload(const HostSlell &h)
+{
+  release();
+  meta = h.view();
+  const size_t nsp = h.slice_ptr.size(), nc = h.cols.size(), ne = h.n_elms();
+  // The reference zero-fills every device allocation (util/cuda/allocator.h:14-20);
+  // here every byte is overwritten by the copy that follows.
+  auto alloc = [](void **p, size_t bytes) -> int {
+    cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+    if (e != cudaSuccess) {
+      *p = nullptr;
+      cudaGetLastError();
+      return fail(e == cudaErrorMemoryAllocation ? ISPM_ERR_NOMEM : ISPM_ERR_CUDA,
+                  "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    }
+    return ISPM_OK;
+  };
+  int st;
+  if ((st = alloc((void **)&slice_ptr, nsp * 4)) || (st = alloc((void **)&cols, nc * 4)) ||
+      (st = alloc(&elms, ne * elm_size(h.elm_dtype)))) {
+    release();
+    return st;
+  }
+  ISPM_CUDA_TRY(cudaMemcpy(slice_ptr, h.slice_ptr.data(), nsp * 4, cudaMemcpyHostToDevice));
+  if (nc)
+    ISPM_CUDA_TRY(cudaMemcpy(cols, h.cols.data(), nc * 4, cudaMemcpyHostToDevice));
+  if (ne)
+    ISPM_CUDA_TRY(
+        cudaMemcpy(elms, h.elms_ptr(), ne * elm_size(h.elm_dtype), cudaMemcpyHostToDevice));
+  return ISPM_OK;
+}
+
+int DeviceSlell::update_elms(const HostSlell &h)
+{
+  if (!elms && meta.n_elms)
+    return fail(ISPM_ERR_INVALID, "device matrix not uploaded");
+  if ((long long)h.n_elms() != meta.n_elms || h.elm_dtype != meta.elm_dtype)
+    return fail(ISPM_ERR_INVALID, "element array shape changed (%zu vs %lld)", h.n_elms(),
+                meta.n_elms);
+  if (meta.n_elms)
+    ISPM_CUDA_TRY(cudaMemcpy(elms, h.elms_ptr(), meta.n_elms * elm_size(h.elm_dtype),
+                             cudaMemcpyHostToDevice));
+  return ISPM_OK;
+}
+
+static unsigned pow2_floor(unsigned v) { return v ? 1u << ilog2(v) : 0u; }
+static unsigned pow2_ceil(unsigned v) { return v <= 1 ? 1u : 1u << (ilog2(v - 1) + 1); }
+
+ispm_launch_params default_launch(int x_dtype, const ispm_slell_view &m)
+{
+  (void)x_dtype;
+  ispm_launch_params p{};
+  const unsigned esz = m.elm_dtype == ISPM_F32 ? 4 : 8;
+  const unsigned hmax = m.var_height ? m.min_slice_height : m.slice_height;
+  unsigned H = 16 / esz;  // one 128-bit load of elements per thread and step
+  while (H > 1 && H > hmax)
+    H >>= 1;
+  const unsigned S = m.var_height ? m.max_slice_height : m.slice_height;
+  unsigned R = S / H ? S / H : 1;
+  // Enough threads to fill the GPU, split a row between several threads
+  // only when rows alone do not.
+  const double avg_width = m.n_rows ? (double)m.n_elms / (double)m.n_rows : 1.0;
+  const double want_threads = 148.0 * 2048.0;
+  const double row_threads = (double)m.n_rows / H;
+  unsigned P = 1;
+  if (row_threads < want_threads)
+    P = pow2_ceil((unsigned)(want_threads / (row_threads > 1 ? row_threads : 1)));
+  unsigned pmax = pow2_floor((unsigned)(avg_width / (m.hblock ? m.hblock : 1)));
+  if (pmax < 1)
+    pmax = 1;
+  if (P > pmax)
+    P = pmax;
+  while (R * P > 1024 && P > 1)
+    P >>= 1;
+  unsigned N = R * P;
+  if (N < 4)
+    N = 4;
+  while (N > 1024 && H < 4 && H * 2 <= hmax) {  // very tall slices: more rows per thread
+    H *= 2;
+    N = (S / H) * P;
+  }
+  p.N = N;
+  p.S = m.var_height ? N * H : m.slice_height;
+  if (m.var_height && p.S < H)
+    p.S = H;
+  p.H = H;
+  p.use_tex_sliceptr = 1;
+  p.use_tex_x = 1;
+  return p;
+}
+
+}  // namespace ispm
+
+using namespace ispm;
+
+extern "C" {
+
+int ispm_initialize(void)
+{
+  clear_error();
+  int dev = 0;
+  ISPM_CUDA_TRY(cudaGetDevice(&dev));
+  int major = 0, minor = 0;
+  ISPM_CUDA_TRY(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+  ISPM_CUDA_TRY(cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev));
+  if (major != 10 || minor != 0)
+    return fail(ISPM_ERR_ARCH, "compiled for sm_100a, device %d is sm_%d%d", dev, major, minor);
+  // The reference sets cudaDeviceMapHost (initialize.cu:28).  Once a context is
+  // active the flag can no longer change; mapped host memory is on by default
+  // with unified addressing, so that refusal is not an error.
+  cudaError_t e = cudaSetDeviceFlags(cudaDeviceMapHost);
+  if (e != cudaSuccess && e != cudaErrorSetOnActiveProcess)
+    return fail(ISPM_ERR_CUDA, "cudaSetDeviceFlags: %s", cudaGetErrorString(e));
+  cudaGetLastError();
+  return ISPM_OK;
+}
+
+int ispm_get_device_string(char *buf, int len)
+{
+  clear_error();
+  if (!buf || len <= 0)
+    return fail(ISPM_ERR_INVALID, "NULL buffer");
+  int dev = 0;
+  ISPM_CUDA_TRY(cudaGetDevice(&dev));
+  cudaDeviceProp p;
+  ISPM_CUDA_TRY(cudaGetDeviceProperties(&p, dev));
+  snprintf(buf, (size_t)len, "%04x:%02x:%02x (%s)", p.pciDomainID, p.pciBusID, p.pciDeviceID,
+           p.name);
+  return ISPM_OK;
+}
+
+int ispm_dslell_upload(const ispm_slell *h, ispm_dslell **out)
+{
+  clear_error();
+  if (!h || !out)
+    return fail(ISPM_ERR_INVALID, "NULL argument");
+  *out = nullptr;
+  ispm_dslell *d = new (std::nothrow) ispm_dslell;
+  if (!d)
+    return fail(ISPM_ERR_NOMEM, "host allocation");
+  int st = d->d.upload(h->m);
+  if (st) {
+    delete d;
+    return st;
+  }
+  *out = d;
+  return ISPM_OK;
+}
+
+int ispm_dslell_update_elms(ispm_dslell *d, const ispm_slell *h)
+{
+  clear_error();
+  if (!d || !h)
+    return fail(ISPM_ERR_INVALID, "NULL argument");
+  return d->d.update_elms(h->m);
+}
+
+int ispm_dslell_get_view(const ispm_dslell *d, ispm_slell_view *view)
+{
+  if (!d || !view)
+    return fail(ISPM_ERR_INVALID, "NULL argument");
+  *view = d->d.view();
+  return ISPM_OK;
+}
+
+void ispm_dslell_free(ispm_dslell *d) { delete d; }
+
+}  // extern "C"

@@ -1,0 +1,342 @@
+// Sliced-ELLPACK SpMV for sm_100a: y = A x.
+//
+// Same matrix layout and launch-parameter meaning as the reference kernel
+// (cuda/spmv/kernel.h:1-135): a slice's entries are column-major (entry
+// (r, k) at slice_start + r + k * slice_height); N threads cooperate on one
+// slice, each covering H consecutive rows, so N * H / slice_height threads
+// share a row and their partial sums are reduced at the end.  What changes
+// for B200:
+//  * several slices per CTA when N is small (the reference runs one slice per
+//    block), so narrow launches still fill the SM;
+//  * matrix words are fetched with 128-bit streaming loads (ld.global.cs)
+//    that do not displace x from L1/L2; x is gathered through the read-only
+//    path with explicit bounds (the reference relied on texture fetches
+//    returning 0 out of range: diagonal-block entries of boundary rows point
+//    one past either end of x);
+//  * the cross-thread reduction is warp shuffles (xor butterfly, uniform
+//    across the warp so slices of different heights may share one) with a
+//    shared-memory step only when a slice spans several warps;
+//  * hblock columns gather W consecutive x values with one vector load.
+#include <cuda_runtime.h>
+
+#include "cuda_util.cuh"
+#include "spmv_launch.h"
+
+namespace ispm {
+namespace {
+
+template <class T, class E> struct SpmvArgs {
+  const unsigned *__restrict__ sp;
+  const unsigned *__restrict__ cols;
+  const E *__restrict__ elms;
+  const T *__restrict__ x;
+  T *__restrict__ y;
+  unsigned n_slices;
+  unsigned slice_height;
+  unsigned n_cols;
+  unsigned tps;       // threads per slice (reference N), power of two
+  unsigned log2_tps;
+  int x_vec_ok;       // x aligned for W-wide vector loads
+};
+
+// Gather x[c*W .. c*W+W-1] into xw, zero beyond n_cols.
+template <class T, int W>
+__device__ __forceinline__ void gather_w(const T *__restrict__ x, unsigned c, unsigned n_cols,
+                                         bool vec_ok, T (&xw)[W])
+{
+  const unsigned base = c * W;
+  if (vec_ok && base + W <= n_cols) {
+    if constexpr (W == 2 && sizeof(T) == 4) {
+      float2 v = __ldg(reinterpret_cast<const float2 *>(x + base));
+      xw[0] = v.x;
+      xw[1] = v.y;
+      return;
+    } else if constexpr (W == 4 && sizeof(T) == 4) {
+      float4 v = __ldg(reinterpret_cast<const float4 *>(x + base));
+      xw[0] = v.x;
+      xw[1] = v.y;
+      xw[2] = v.z;
+      xw[3] = v.w;
+      return;
+    } else if constexpr (W == 2 && sizeof(T) == 8) {
+      double2 v = __ldg(reinterpret_cast<const double2 *>(x + base));
+      xw[0] = v.x;
+      xw[1] = v.y;
+      return;
+    } else if constexpr (W == 4 && sizeof(T) == 8) {
+      double2 a = __ldg(reinterpret_cast<const double2 *>(x + base));
+      double2 b = __ldg(reinterpret_cast<const double2 *>(x + base + 2));
+      xw[0] = a.x;
+      xw[1] = a.y;
+      xw[2] = b.x;
+      xw[3] = b.y;
+      return;
+    }
+  }
+#pragma unroll
+  for (int w = 0; w < W; w++)
+    xw[w] = ld_x_guard(x, base + w, n_cols);
+}
+
+template <class T, class E, int H, int W, bool VAR, bool DIAG>
+__global__ void __launch_bounds__(1024) slell_spmv_kernel(SpmvArgs<T, E> a)
+{
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr unsigned spe = 1 + (W > 1) + (VAR ? 1 : 0) + (DIAG ? 2 : 0);
+  const unsigned tps = a.tps;
+  const unsigned t = threadIdx.x & (tps - 1);
+  const unsigned slice_in_cta = threadIdx.x >> a.log2_tps;
+  const unsigned b = blockIdx.x * (blockDim.x >> a.log2_tps) + slice_in_cta;
+  const bool active = b < a.n_slices;
+
+  // Slice header (kernel.h:13-61); inactive slices walk nothing.
+  unsigned e0 = 0, e1 = 0, c0 = 0, c1 = 0, cb = 0, d0 = 0, y0 = 0;
+  unsigned sz = VAR ? tps * H : a.slice_height;
+  if (active) {
+    const unsigned *rec = a.sp + (size_t)spe * b;
+    e0 = __ldg(rec);
+    e1 = __ldg(rec + spe);
+    if (VAR) {
+      y0 = __ldg(rec + 1);
+      sz = __ldg(rec + 1 + spe) - y0;
+    } else {
+      y0 = b * a.slice_height;
+    }
+    if constexpr (DIAG) {
+      c0 = __ldg(rec + (VAR ? 2 : 1));
+      d0 = __ldg(rec + (VAR ? 3 : 2));
+      c1 = __ldg(rec + (VAR ? 2 : 1) + spe);
+    } else if constexpr (W > 1) {
+      c0 = __ldg(rec + (VAR ? 2 : 1));
+      c1 = __ldg(rec + (VAR ? 2 : 1) + spe);
+      const unsigned nse = (W * (c1 - c0) - (e1 - e0)) / (W - 1);
+      cb = c1;
+      c1 = c0 + nse;
+      e1 = e0 + nse;
+    } else {
+      c0 = e0;
+      c1 = e1;
+    }
+  }
+
+  const unsigned step = tps * H;
+  T acc[H];
+#pragma unroll
+  for (int h = 0; h < H; h++)
+    acc[h] = T(0);
+
+  unsigned i = e0 + t * H, j = c0 + t * H;
+  // ELL part with explicit columns (kernel.h:70-79).
+#pragma unroll 4
+  for (; j < c1; i += step, j += step) {
+    Vec<H, unsigned> cc = ld_stream<H>(a.cols + j);
+    Vec<H, E> ee = ld_stream<H>(a.elms + i);
+#pragma unroll
+    for (int h = 0; h < H; h++)
+      acc[h] = fma(T(ee.v[h]), ld_x_guard(a.x, cc.v[h], a.n_cols), acc[h]);
+  }
+  if constexpr (DIAG) {
+    // Diagonal blocks (kernel.h:80-92): column index = diag_pos + row - sz.
+    const unsigned adj = ((t * H) & (sz - 1)) - sz;
+    unsigned jj = d0 + (j - c1) / sz;
+    const unsigned jstep = step / sz;
+#pragma unroll 4
+    for (; i < e1; i += step, jj += jstep) {
+      const unsigned base = __ldg(a.sp + jj) + adj;
+      Vec<H, E> ee = ld_stream<H>(a.elms + i);
+#pragma unroll
+      for (int h = 0; h < H; h++)
+        acc[h] = fma(T(ee.v[h]), ld_x_guard(a.x, base + h, a.n_cols), acc[h]);
+    }
+  } else if constexpr (W > 1) {
+    // hblock columns (kernel.h:93-119): W values per stored column index.
+    i = e1 + ((i - e1) & (sz - 1)) + ((i - e1) & ~(sz - 1)) * W;
+    const bool vec_ok = a.x_vec_ok;
+#pragma unroll 2
+    for (; j < cb; i += W * step, j += step) {
+      Vec<H, unsigned> cc = ld_stream<H>(a.cols + j);
+      Vec<H, E> ew[W];
+#pragma unroll
+      for (int w = 0; w < W; w++)
+        ew[w] = ld_stream<H>(a.elms + i + w * sz);
+#pragma unroll
+      for (int h = 0; h < H; h++) {
+        T xw[W];
+        gather_w<T, W>(a.x, cc.v[h], a.n_cols, vec_ok, xw);
+#pragma unroll
+        for (int w = 0; w < W; w++)
+          acc[h] = fma(T(ew[w].v[h]), xw[w], acc[h]);
+      }
+    }
+  }
+
+  // Reduce the partial sums of the threads sharing a row (reduce.h:80-127).
+  const unsigned R = sz / H;  // row groups in this slice
+  const unsigned wspan = tps < 32 ? tps : 32;
+  for (unsigned off = 1; off < wspan; off <<= 1) {
+#pragma unroll
+    for (int h = 0; h < H; h++) {
+      T v = __shfl_xor_sync(0xffffffffu, acc[h], off);
+      if (off >= R)
+        acc[h] += v;
+    }
+  }
+  if (tps > 32) {
+    T *red = reinterpret_cast<T *>(smem_raw);
+#pragma unroll
+    for (int h = 0; h < H; h++)
+      red[threadIdx.x * H + h] = acc[h];
+    __syncthreads();
+    if (t < R) {
+      const unsigned stride = R > 32 ? R : 32;
+      const unsigned base = slice_in_cta * tps;
+#pragma unroll
+      for (int h = 0; h < H; h++) {
+        T s = T(0);
+        for (unsigned k = t; k < tps; k += stride)
+          s += red[(base + k) * H + h];
+        acc[h] = s;
+      }
+    }
+  }
+  if (active && t < R)
+    st_vec<H, T>(a.y + y0 + t * H, acc);
+}
+
+template <class T, class E, int H, int W, bool VAR, bool DIAG>
+int launch_one(const SpmvArgs<T, E> &args, unsigned tps, cudaStream_t stream)
+{
+  const unsigned block = tps >= 256 ? tps : 256;
+  const unsigned spb = block / tps;
+  const unsigned grid = (args.n_slices + spb - 1) / spb;
+  const size_t smem = tps > 32 ? (size_t)block * H * sizeof(T) : 0;
+  slell_spmv_kernel<T, E, H, W, VAR, DIAG><<<grid, block, smem, stream>>>(args);
+  cudaError_t e = cudaPeekAtLastError();
+  if (e != cudaSuccess)
+    return fail(ISPM_ERR_CUDA, "SpMV launch: %s", cudaGetErrorString(e));
+  return ISPM_OK;
+}
+
+template <class T, class E, int H>
+int launch_h(const SpmvArgs<T, E> &args, const ispm_slell_view &m, unsigned tps,
+             cudaStream_t s)
+{
+  const bool V = m.var_height != 0, D = m.diags != 0;
+  switch (m.hblock) {
+  case 1:
+    if (V)
+      return D ? launch_one<T, E, H, 1, true, true>(args, tps, s)
+               : launch_one<T, E, H, 1, true, false>(args, tps, s);
+    return D ? launch_one<T, E, H, 1, false, true>(args, tps, s)
+             : launch_one<T, E, H, 1, false, false>(args, tps, s);
+  case 2:
+    return V ? launch_one<T, E, H, 2, true, false>(args, tps, s)
+             : launch_one<T, E, H, 2, false, false>(args, tps, s);
+  case 4:
+    return V ? launch_one<T, E, H, 4, true, false>(args, tps, s)
+             : launch_one<T, E, H, 4, false, false>(args, tps, s);
+  }
+  return fail(ISPM_ERR_INVALID, "hblock %u", m.hblock);
+}
+
+template <class T, class E>
+int launch_te(const ispm_launch_params &p, const ispm_slell_view &m, const void *x, void *y,
+              cudaStream_t s)
+{
+  SpmvArgs<T, E> a;
+  a.sp = m.slice_ptr;
+  a.cols = m.cols;
+  a.elms = static_cast<const E *>(m.elms);
+  a.x = static_cast<const T *>(x);
+  a.y = static_cast<T *>(y);
+  a.n_slices = m.n_slices;
+  a.slice_height = m.slice_height;
+  a.n_cols = (unsigned)m.n_cols;
+  a.tps = p.N;
+  a.log2_tps = (unsigned)ilog2(p.N);
+  a.x_vec_ok = aligned(x, (size_t)m.hblock * sizeof(T));
+  if (!aligned(m.elms, p.H * sizeof(E)) || !aligned(m.cols, p.H * sizeof(unsigned)) ||
+      !aligned(y, p.H * sizeof(T)))
+    return fail(ISPM_ERR_INVALID, "matrix arrays or y not aligned to H=%u elements", p.H);
+  switch (p.H) {
+  case 1: return launch_h<T, E, 1>(a, m, p.N, s);
+  case 2: return launch_h<T, E, 2>(a, m, p.N, s);
+  case 4: return launch_h<T, E, 4>(a, m, p.N, s);
+  }
+  return fail(ISPM_ERR_INVALID, "H %u", p.H);
+}
+
+}  // namespace
+
+int check_launch(int x_dtype, const ispm_launch_params &p, const ispm_slell_view &m)
+{
+  const int e = m.elm_dtype;
+  if (!((x_dtype == ISPM_F32 && e == ISPM_F32) || (x_dtype == ISPM_F64 && e == ISPM_F32) ||
+        (x_dtype == ISPM_F64 && e == ISPM_F64)))
+    return fail(ISPM_ERR_INVALID, "(T, E) = (%s, %s) is not an instantiated pair",
+                x_dtype == ISPM_F64 ? "double" : "float", e == ISPM_F64 ? "double" : "float");
+  if (!is_pow2(p.N) || p.N < 4 || p.N > 1024)
+    return fail(ISPM_ERR_INVALID, "N = %u (power of two in [4, 1024])", p.N);
+  if (p.H != 1 && p.H != 2 && p.H != 4)
+    return fail(ISPM_ERR_INVALID, "H = %u (1, 2 or 4)", p.H);
+  if (!(p.N >= p.S / p.H && p.S >= p.H))
+    return fail(ISPM_ERR_INVALID, "launch params fail N >= S/H && S >= H");
+  if (m.hblock != 1 && m.hblock != 2 && m.hblock != 4)
+    return fail(ISPM_ERR_INVALID, "hblock %u", m.hblock);
+  if (m.diags && m.hblock > 1)
+    return fail(ISPM_ERR_INVALID, "diagonal blocks with hblock > 1");
+  if (m.n_slices == 0)
+    return ISPM_OK;
+  if (!m.var_height) {
+    if (p.S != m.slice_height)
+      return fail(ISPM_ERR_INVALID, "S = %u but the matrix slice height is %u", p.S,
+                  m.slice_height);
+    if (!is_pow2(m.slice_height))
+      return fail(ISPM_ERR_INVALID, "slice height %u is not a power of two", m.slice_height);
+  } else {
+    if (!is_pow2(m.min_slice_height) || !is_pow2(m.max_slice_height))
+      return fail(ISPM_ERR_INVALID, "variable slice heights must be powers of two");
+    if (m.min_slice_height < p.H)
+      return fail(ISPM_ERR_INVALID, "H = %u exceeds the shortest slice (%u rows)", p.H,
+                  m.min_slice_height);
+    if ((unsigned long long)p.N * p.H < m.max_slice_height)
+      return fail(ISPM_ERR_INVALID, "N*H = %u below the tallest slice (%u rows)", p.N * p.H,
+                  m.max_slice_height);
+  }
+  return ISPM_OK;
+}
+
+int launch_spmv(int x_dtype, const ispm_launch_params &p, const ispm_slell_view &m,
+                const void *x, void *y, cudaStream_t s)
+{
+  int st = check_launch(x_dtype, p, m);
+  if (st || m.n_slices == 0)
+    return st;
+  if (!x || !y || !m.slice_ptr || (m.n_elms && (!m.elms)) || (m.n_cols_arr && !m.cols))
+    return fail(ISPM_ERR_INVALID, "NULL pointer");
+  if (x_dtype == ISPM_F32)
+    return launch_te<float, float>(p, m, x, y, s);
+  if (m.elm_dtype == ISPM_F32)
+    return launch_te<double, float>(p, m, x, y, s);
+  return launch_te<double, double>(p, m, x, y, s);
+}
+
+}  // namespace ispm
+
+extern "C" {
+
+int ispm_launch_params_valid(const ispm_launch_params *p)
+{
+  return p && p->H && p->N >= p->S / p->H && p->S >= p->H;
+}
+
+int ispm_launch_spmv(int x_dtype, const ispm_launch_params *p, const ispm_slell_view *m,
+                     const void *x, void *y, void *stream)
+{
+  ispm::clear_error();
+  if (!p || !m)
+    return ispm::fail(ISPM_ERR_INVALID, "NULL params or matrix");
+  return ispm::launch_spmv(x_dtype, *p, *m, x, y, (cudaStream_t)stream);
+}
+
+}  // extern "C"

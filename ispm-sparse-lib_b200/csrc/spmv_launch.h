@@ -1,0 +1,46 @@
+// Internal SpMV launch interface (used by the C ABI, the plan and the solver).
+#ifndef ISPM_SPMV_LAUNCH_H
+#define ISPM_SPMV_LAUNCH_H
+
+#include <cuda_runtime.h>
+
+#include "ispm_internal.h"
+
+namespace ispm {
+
+// Validate launch parameters against a matrix (no CUDA calls).
+int check_launch(int x_dtype, const ispm_launch_params &p, const ispm_slell_view &m);
+// Validate and launch y = A x on `s`.
+int launch_spmv(int x_dtype, const ispm_launch_params &p, const ispm_slell_view &m,
+                const void *x, void *y, cudaStream_t s);
+
+// Device-resident sliced-ELL matrix.
+struct DeviceSlell {
+  ispm_slell_view meta{};  // host copy of the metadata; pointers are device pointers
+  unsigned *slice_ptr = nullptr;
+  unsigned *cols = nullptr;
+  void *elms = nullptr;
+  ispm_slell_view view() const
+  {
+    ispm_slell_view v = meta;
+    v.slice_ptr = slice_ptr;
+    v.cols = cols;
+    v.elms = elms;
+    return v;
+  }
+  int upload(const HostSlell &h);
+  int update_elms(const HostSlell &h);
+  void release();
+  ~DeviceSlell() { release(); }
+};
+
+// B200 launch heuristic for a matrix: threads per slice and rows per thread.
+ispm_launch_params default_launch(int x_dtype, const ispm_slell_view &m);
+
+}  // namespace ispm
+
+struct ispm_dslell {
+  ispm::DeviceSlell d;
+};
+
+#endif

@@ -1,0 +1,560 @@
+"""Python mirror of the ispm-sparse-lib hot-path API over the C ABI.
+
+Names follow the reference's C++ API (formats/formats.h, formats/conversion.h,
+plan/plan.h, fastainv/fastainv.h, cuda/spmv/kernel-iface.h, util/cuda/sblas.h,
+fastainv/droptol-tuning.h, util/cuda/initialize.h) so that code written against
+it reads like the reference's.  Everything computes in libispm_b200.so; this
+module only marshals arguments.  Device vectors are passed as torch CUDA
+tensors (device memory and streams only -- no torch kernels are used on the
+path), or as raw device pointers (ints).
+
+Error behaviour: every C-ABI status other than ISPM_OK raises IspmError; the
+reference aborts on CUDA errors and silently ignores unsupported launch
+parameters, both of which surface here as exceptions instead.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_PKG = os.path.dirname(_HERE)
+LIB_PATH = os.path.join(_PKG, "libispm_b200.so")
+
+F32, F64 = 0, 1
+OK = 0
+ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_ARCH = 1, 2, 3, 4
+ERR_BREAKDOWN, ERR_NOT_CONVERGED, ERR_TIMEOUT, ERR_TOO_LARGE = 5, 6, 7, 8
+
+PLAN_DEFAULT, PLAN_ESTIMATE, PLAN_EXHAUSTIVE = 0, 1, 2
+SPMV_NO_TEXTURE_MEMORY, SPMV_PLAN_NO_DEVICE = 1, 2
+
+_NP = {F32: np.float32, F64: np.float64}
+
+
+class IspmError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+
+
+class slell_view(C.Structure):
+    _fields_ = [
+        ("n_rows", C.c_int), ("n_cols", C.c_int), ("n_nz", C.c_int),
+        ("slice_height", C.c_uint), ("n_slices", C.c_uint), ("hblock", C.c_uint),
+        ("var_height", C.c_int), ("diags", C.c_int), ("elm_dtype", C.c_int),
+        ("min_slice_height", C.c_uint), ("max_slice_height", C.c_uint),
+        ("n_slice_ptr", C.c_longlong), ("n_cols_arr", C.c_longlong), ("n_elms", C.c_longlong),
+        ("slice_ptr", C.c_void_p), ("cols", C.c_void_p), ("elms", C.c_void_p),
+    ]
+
+
+class slell_params(C.Structure):
+    _fields_ = [("S", C.c_uint), ("H", C.c_uint), ("V", C.c_uint), ("D", C.c_uint)]
+
+
+class spmv_launch_params(C.Structure):
+    """cuda/spmv/kernel-iface.h:6-17"""
+    _fields_ = [("N", C.c_uint), ("S", C.c_uint), ("H", C.c_uint),
+                ("use_tex_sliceptr", C.c_int), ("use_tex_x", C.c_int)]
+
+    def valid(self) -> bool:
+        return bool(_lib().ispm_launch_params_valid(C.byref(self)))
+
+    def __repr__(self):
+        return f"spmv_launch_params(N={self.N}, S={self.S}, H={self.H})"
+
+
+class fastainv_stats(C.Structure):
+    _fields_ = [("storage_chunks", C.c_longlong), ("chunks_used", C.c_longlong),
+                ("truncated_rows", C.c_longlong), ("breakdowns", C.c_longlong)]
+
+
+_L = None
+
+
+def _lib():
+    global _L
+    if _L is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `make -C {_PKG}` "
+                "(there is no fallback implementation)")
+        _L = C.CDLL(LIB_PATH)
+        _declare(_L)
+    return _L
+
+
+def lib_handle():
+    """The loaded libispm_b200.so (ctypes.CDLL)."""
+    return _lib()
+
+
+def _declare(L):
+    vp, i, u, d, ll = C.c_void_p, C.c_int, C.c_uint, C.c_double, C.c_longlong
+    ip = C.POINTER(C.c_int)
+    sig = {
+        "ispm_error_string": (C.c_char_p, [i]),
+        "ispm_last_error": (C.c_char_p, []),
+        "ispm_version": (C.c_char_p, []),
+        "ispm_initialize": (i, []),
+        "ispm_get_device_string": (i, [C.c_char_p, i]),
+        "ispm_csr_to_slell": (i, [i, i, i, vp, vp, vp, i, i, i, i, i, C.POINTER(vp)]),
+        "ispm_csr_to_slell_guess_format": (i, [i, i, i, vp, vp, vp, i, i, C.POINTER(vp)]),
+        "ispm_slell_get_view": (i, [vp, C.POINTER(slell_view)]),
+        "ispm_slell_elms": (vp, [vp]),
+        "ispm_slell_spmv_bytes": (C.c_ulonglong, [vp, i, i]),
+        "ispm_slell_free": (None, [vp]),
+        "ispm_dslell_upload": (i, [vp, C.POINTER(vp)]),
+        "ispm_dslell_update_elms": (i, [vp, vp]),
+        "ispm_dslell_get_view": (i, [vp, C.POINTER(slell_view)]),
+        "ispm_dslell_free": (None, [vp]),
+        "ispm_launch_params_valid": (i, [C.POINTER(spmv_launch_params)]),
+        "ispm_launch_spmv": (i, [i, C.POINTER(spmv_launch_params), C.POINTER(slell_view),
+                                 vp, vp, vp]),
+        "ispm_plan_create": (i, [i, i, i, i, vp, vp, vp, i, u, C.POINTER(vp)]),
+        "ispm_plan_execute": (i, [vp, vp, vp, vp]),
+        "ispm_plan_upload": (i, [vp]),
+        "ispm_plan_update_device_matrix_coefs": (i, [vp]),
+        "ispm_plan_change_host_matrix": (i, [vp, i, i, vp, vp, vp]),
+        "ispm_plan_get_params": (i, [vp, C.POINTER(slell_params),
+                                     C.POINTER(spmv_launch_params)]),
+        "ispm_plan_host_matrix": (vp, [vp]),
+        "ispm_plan_device_matrix": (vp, [vp]),
+        "ispm_plan_tuned_seconds": (d, [vp]),
+        "ispm_plan_free": (None, [vp]),
+        "ispm_sblas_copy_indexed": (i, [i, vp, vp, vp, i, vp]),
+        "ispm_sblas_add_indexed": (i, [i, vp, vp, vp, i, vp]),
+        "ispm_sblas_dot": (i, [i, vp, vp, vp, i, vp]),
+        "ispm_sblas_ppcg_update_scalars": (i, [i, vp, vp, vp, vp, vp, vp]),
+        "ispm_sblas_ppcg_update_vectors": (i, [i] + [vp] * 15 + [i, vp]),
+        "ispm_fastainv_sym": (i, [i, i, vp, vp, vp, vp, vp, ll, d, C.POINTER(vp),
+                                  C.POINTER(vp), C.POINTER(fastainv_stats)]),
+        "ispm_csr_get_info": (i, [vp, ip, ip, ip, ip]),
+        "ispm_csr_get_arrays": (i, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
+        "ispm_csr_free": (None, [vp]),
+        "ispm_droptol_tuner_create": (vp, [d, d]),
+        "ispm_droptol_tuner_get_droptol": (d, [vp]),
+        "ispm_droptol_tuner_get_best_droptol": (d, [vp]),
+        "ispm_droptol_tuner_note_time": (None, [vp, d]),
+        "ispm_droptol_tuner_restart": (None, [vp]),
+        "ispm_droptol_tuner_reset_phase": (None, [vp]),
+        "ispm_droptol_tuner_iterations": (i, [vp]),
+        "ispm_droptol_tuner_free": (None, [vp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+
+
+def _check(status: int):
+    if status != OK:
+        msg = _lib().ispm_last_error().decode() or _lib().ispm_error_string(status).decode()
+        raise IspmError(status, msg)
+
+
+def _ptr(a):
+    """Address of a numpy array, torch tensor or raw int pointer."""
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return a
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    raise TypeError(f"cannot take the address of {type(a)}")
+
+
+def _dtype_code(a) -> int:
+    if isinstance(a, np.ndarray):
+        dt = a.dtype
+    else:
+        dt = getattr(a, "dtype", None)
+    s = str(dt)
+    if s.endswith("float32"):
+        return F32
+    if s.endswith("float64"):
+        return F64
+    raise TypeError(f"unsupported element type {dt}")
+
+
+def _stream(stream):
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream  # torch.cuda.Stream
+
+
+# ---------------------------------------------------------------------------
+# util/cuda/initialize.h
+# ---------------------------------------------------------------------------
+
+def ispm_initialize():
+    _check(_lib().ispm_initialize())
+
+
+def get_device_string() -> str:
+    buf = C.create_string_buffer(64)
+    _check(_lib().ispm_get_device_string(buf, 64))
+    return buf.value.decode()
+
+
+def version() -> str:
+    return _lib().ispm_version().decode()
+
+
+# ---------------------------------------------------------------------------
+# formats/formats.h
+# ---------------------------------------------------------------------------
+
+class csr_matrix:
+    """formats/formats.h:18-37 (host CSR): row_ptr int32[n+1], cols int32[nnz],
+    elms float32/float64[nnz]."""
+
+    def __init__(self, n_rows, n_cols, row_ptr, cols, elms):
+        self.n_rows = int(n_rows)
+        self.n_cols = int(n_cols)
+        self.row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int32)
+        self.cols = np.ascontiguousarray(cols, dtype=np.int32)
+        self.elms = np.ascontiguousarray(elms)
+        if self.elms.dtype not in (np.float32, np.float64):
+            self.elms = self.elms.astype(np.float64)
+        self.n_nz = int(self.row_ptr[-1])
+
+    def pad(self, k: int):
+        """formats.h:23-30: append empty rows up to a multiple of k (in place)."""
+        n_pad = (self.n_rows + k - 1) // k * k
+        if n_pad > self.n_rows:
+            self.row_ptr = np.concatenate(
+                [self.row_ptr, np.full(n_pad - self.n_rows, self.row_ptr[-1], np.int32)])
+            self.n_rows = n_pad
+
+    def spmv_bytes(self) -> int:
+        """formats.h:32-36"""
+        return 4 * (self.row_ptr.size + self.cols.size) + self.elms.itemsize * (
+            self.elms.size + 2 * self.n_rows)
+
+    def astype(self, dtype):
+        return csr_matrix(self.n_rows, self.n_cols, self.row_ptr, self.cols,
+                          self.elms.astype(dtype))
+
+    def to_scipy(self):
+        import scipy.sparse as sp
+        return sp.csr_matrix((self.elms, self.cols, self.row_ptr),
+                             shape=(self.n_rows, self.n_cols))
+
+
+class slell_matrix:
+    """Host sliced-ELL matrix (formats/formats.h:44-102), owned by the library."""
+
+    def __init__(self, handle, owner=True, keepalive=None):
+        self._h = C.c_void_p(handle)
+        self._owner = owner
+        self._keep = keepalive
+
+    def __del__(self):
+        if getattr(self, "_owner", False) and self._h and _L is not None:
+            _L.ispm_slell_free(self._h)
+            self._h = None
+
+    def view(self) -> slell_view:
+        v = slell_view()
+        _check(_lib().ispm_slell_get_view(self._h, C.byref(v)))
+        return v
+
+    def __getattr__(self, name):
+        if name in ("n_rows", "n_cols", "n_nz", "slice_height", "n_slices", "hblock",
+                    "var_height", "diags", "elm_dtype", "min_slice_height",
+                    "max_slice_height"):
+            return getattr(self.view(), name)
+        raise AttributeError(name)
+
+    def _arr(self, ptr, n, dtype):
+        if n == 0:
+            return np.zeros(0, dtype)
+        buf = (C.c_char * (n * np.dtype(dtype).itemsize)).from_address(ptr)
+        return np.frombuffer(buf, dtype=dtype, count=n)
+
+    @property
+    def slice_ptr(self):
+        v = self.view()
+        return self._arr(v.slice_ptr, v.n_slice_ptr, np.uint32).copy()
+
+    @property
+    def cols(self):
+        v = self.view()
+        return self._arr(v.cols, v.n_cols_arr, np.uint32).copy()
+
+    @property
+    def elms(self):
+        """Live (writable) view of the host element array."""
+        v = self.view()
+        return self._arr(_lib().ispm_slell_elms(self._h), v.n_elms, _NP[v.elm_dtype])
+
+    def spmv_bytes(self, effective=False, vec_elt_size=None):
+        v = self.view()
+        if vec_elt_size is None:
+            vec_elt_size = 4 if v.elm_dtype == F32 else 8
+        return int(_lib().ispm_slell_spmv_bytes(self._h, int(effective), int(vec_elt_size)))
+
+    def upload(self) -> "device_slell_matrix":
+        """slell_matrix<E, device>(host) (formats.h:56-66)."""
+        out = C.c_void_p()
+        _check(_lib().ispm_dslell_upload(self._h, C.byref(out)))
+        return device_slell_matrix(out.value, owner=True)
+
+
+class device_slell_matrix:
+    """Device sliced-ELL matrix (slell_matrix<E, device_memory_space_tag>)."""
+
+    def __init__(self, handle, owner=True, keepalive=None):
+        self._h = C.c_void_p(handle)
+        self._owner = owner
+        self._keep = keepalive
+
+    def __del__(self):
+        if getattr(self, "_owner", False) and self._h and _L is not None:
+            _L.ispm_dslell_free(self._h)
+            self._h = None
+
+    def view(self) -> slell_view:
+        v = slell_view()
+        _check(_lib().ispm_dslell_get_view(self._h, C.byref(v)))
+        return v
+
+    def update_elms(self, host: slell_matrix):
+        _check(_lib().ispm_dslell_update_elms(self._h, host._h))
+
+    def __getattr__(self, name):
+        if name in ("n_rows", "n_cols", "n_nz", "slice_height", "n_slices", "hblock",
+                    "var_height", "diags", "elm_dtype", "min_slice_height",
+                    "max_slice_height"):
+            return getattr(self.view(), name)
+        raise AttributeError(name)
+
+
+# ---------------------------------------------------------------------------
+# formats/conversion.h
+# ---------------------------------------------------------------------------
+
+def csr_to_slell(A: csr_matrix, req_slice_height: int, hblock: int, var_height: bool,
+                 use_diags: bool, min_height: int = 4) -> slell_matrix:
+    """conversion.h:338-414.  Like the reference, pads A to a multiple of 512
+    rows in place (conversion.h:343)."""
+    code = _dtype_code(A.elms)
+    out = C.c_void_p()
+    _check(_lib().ispm_csr_to_slell(code, A.n_rows, A.n_cols, _ptr(A.row_ptr), _ptr(A.cols),
+                                    _ptr(A.elms), int(req_slice_height), int(hblock),
+                                    int(bool(var_height)), int(bool(use_diags)),
+                                    int(min_height), C.byref(out)))
+    A.pad(512)
+    return slell_matrix(out.value)
+
+
+def csr_to_slell_guess_format(A: csr_matrix, examine_ratio: int = 1,
+                              min_height: int = 4) -> slell_matrix:
+    """conversion.h:416-492"""
+    code = _dtype_code(A.elms)
+    out = C.c_void_p()
+    _check(_lib().ispm_csr_to_slell_guess_format(code, A.n_rows, A.n_cols, _ptr(A.row_ptr),
+                                                 _ptr(A.cols), _ptr(A.elms),
+                                                 int(examine_ratio), int(min_height),
+                                                 C.byref(out)))
+    A.pad(512)
+    return slell_matrix(out.value)
+
+
+# ---------------------------------------------------------------------------
+# cuda/spmv/kernel-iface.h
+# ---------------------------------------------------------------------------
+
+def launch_spmv_kernel(params: spmv_launch_params, m, x, y, stream=None):
+    """launch_spmv_kernel<T, E>(params, m, x, y): T from x's dtype, E from m."""
+    v = m.view() if hasattr(m, "view") else m
+    _check(_lib().ispm_launch_spmv(_dtype_code(x), C.byref(params), C.byref(v), _ptr(x),
+                                   _ptr(y), _stream(stream)))
+
+
+# ---------------------------------------------------------------------------
+# plan/plan.h
+# ---------------------------------------------------------------------------
+
+class spmv_plan:
+    """spmv_plan<T, E> (plan/plan.h:20-161).  T is the vector type, E the
+    matrix element type (taken from the CSR)."""
+
+    def __init__(self, m: csr_matrix, kind: int = PLAN_DEFAULT, flags: int = 0, T=None):
+        edt = _dtype_code(m.elms)
+        vdt = edt if T is None else (F64 if np.dtype(T) == np.float64 else F32)
+        out = C.c_void_p()
+        _check(_lib().ispm_plan_create(vdt, edt, m.n_rows, m.n_cols, _ptr(m.row_ptr),
+                                       _ptr(m.cols), _ptr(m.elms), int(kind), int(flags),
+                                       C.byref(out)))
+        self._h = out
+        self.vec_dtype = vdt
+        self.elm_dtype = edt
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _L is not None:
+            _L.ispm_plan_free(self._h)
+            self._h = None
+
+    def execute_spmv(self, x, y, stream=None):
+        _check(_lib().ispm_plan_execute(self._h, _ptr(x), _ptr(y), _stream(stream)))
+
+    def upload(self):
+        _check(_lib().ispm_plan_upload(self._h))
+
+    def update_device_matrix_coefs(self):
+        _check(_lib().ispm_plan_update_device_matrix_coefs(self._h))
+
+    def change_host_matrix(self, m: csr_matrix):
+        _check(_lib().ispm_plan_change_host_matrix(self._h, m.n_rows, m.n_cols,
+                                                   _ptr(m.row_ptr), _ptr(m.cols),
+                                                   _ptr(m.elms)))
+
+    @property
+    def mparams(self) -> slell_params:
+        mp, p = slell_params(), spmv_launch_params()
+        _check(_lib().ispm_plan_get_params(self._h, C.byref(mp), C.byref(p)))
+        return mp
+
+    @property
+    def params(self) -> spmv_launch_params:
+        mp, p = slell_params(), spmv_launch_params()
+        _check(_lib().ispm_plan_get_params(self._h, C.byref(mp), C.byref(p)))
+        return p
+
+    @property
+    def host_matrix(self):
+        h = _lib().ispm_plan_host_matrix(self._h)
+        return slell_matrix(h, owner=False, keepalive=self) if h else None
+
+    @property
+    def device_matrix(self):
+        h = _lib().ispm_plan_device_matrix(self._h)
+        return device_slell_matrix(h, owner=False, keepalive=self) if h else None
+
+    @property
+    def tuned_seconds(self) -> float:
+        return float(_lib().ispm_plan_tuned_seconds(self._h))
+
+
+# ---------------------------------------------------------------------------
+# fastainv/fastainv.h
+# ---------------------------------------------------------------------------
+
+_PROGRESS = C.CFUNCTYPE(None, C.c_void_p)
+
+
+def _csr_from_handle(h) -> csr_matrix:
+    L = _lib()
+    nr, nc, nz, dt = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    _check(L.ispm_csr_get_info(h, C.byref(nr), C.byref(nc), C.byref(nz), C.byref(dt)))
+    rp, ci, el = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    _check(L.ispm_csr_get_arrays(h, C.byref(rp), C.byref(ci), C.byref(el)))
+    n, nnz = nr.value, nz.value
+    npdt = _NP[dt.value]
+
+    def arr(p, count, t):
+        if count == 0:
+            return np.zeros(0, t)
+        return np.frombuffer((C.c_char * (count * np.dtype(t).itemsize)).from_address(p),
+                             dtype=t, count=count).copy()
+
+    out = csr_matrix(n, nc.value, arr(rp.value, n + 1, np.int32), arr(ci.value, nnz, np.int32),
+                     arr(el.value, nnz, npdt))
+    L.ispm_csr_free(h)
+    return out
+
+
+def fastainv_sym(A: csr_matrix, out_dtype=np.float64, progress=None,
+                 max_elts: int = 8192000, droptol: float = 0.125, stats=None):
+    """fastainv_sym<double, out_real>(Ainv1, Ainv2, A, progress, v, max_elts,
+    droptol) (fastainv/fastainv.h:8-30).  Returns (Ainv1, Ainv2)."""
+    if A.elms.dtype != np.float64:
+        raise TypeError("fastainv_sym takes an FP64 CSR (csr_matrix<double>)")
+    odt = F64 if np.dtype(out_dtype) == np.float64 else F32
+    cb = _PROGRESS(lambda _v: progress()) if progress else None
+    g1, g2 = C.c_void_p(), C.c_void_p()
+    st = fastainv_stats()
+    _check(_lib().ispm_fastainv_sym(odt, A.n_rows, _ptr(A.row_ptr), _ptr(A.cols),
+                                    _ptr(A.elms), C.cast(cb, C.c_void_p) if cb else None,
+                                    None, int(max_elts), float(droptol), C.byref(g1),
+                                    C.byref(g2), C.byref(st)))
+    if stats is not None:
+        stats.update({k: getattr(st, k) for k, _ in fastainv_stats._fields_})
+    return _csr_from_handle(g1), _csr_from_handle(g2)
+
+
+# ---------------------------------------------------------------------------
+# fastainv/droptol-tuning.h
+# ---------------------------------------------------------------------------
+
+class DroptolTuner:
+    def __init__(self, lo: float = -10, hi: float = -3):
+        self._h = C.c_void_p(_lib().ispm_droptol_tuner_create(float(lo), float(hi)))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _L is not None:
+            _L.ispm_droptol_tuner_free(self._h)
+            self._h = None
+
+    def getDroptol(self) -> float:
+        return _lib().ispm_droptol_tuner_get_droptol(self._h)
+
+    def getBestDroptol(self) -> float:
+        return _lib().ispm_droptol_tuner_get_best_droptol(self._h)
+
+    def noteTime(self, t: float):
+        _lib().ispm_droptol_tuner_note_time(self._h, float(t))
+
+    def restart(self):
+        _lib().ispm_droptol_tuner_restart(self._h)
+
+    def resetPhase(self):
+        _lib().ispm_droptol_tuner_reset_phase(self._h)
+
+    def iterations(self) -> int:
+        return _lib().ispm_droptol_tuner_iterations(self._h)
+
+
+# ---------------------------------------------------------------------------
+# util/cuda/sblas.h (device pointers / CUDA tensors)
+# ---------------------------------------------------------------------------
+
+class sblas:
+    @staticmethod
+    def copy_indexed(dst, src, i, n_elts, stream=None):
+        _check(_lib().ispm_sblas_copy_indexed(_dtype_code(dst), _ptr(dst), _ptr(src), _ptr(i),
+                                              int(n_elts), _stream(stream)))
+
+    @staticmethod
+    def add_indexed(dst, src, i, n_elts, stream=None):
+        _check(_lib().ispm_sblas_add_indexed(_dtype_code(dst), _ptr(dst), _ptr(src), _ptr(i),
+                                             int(n_elts), _stream(stream)))
+
+    @staticmethod
+    def dot(x, y, s, n_elts, stream=None):
+        _check(_lib().ispm_sblas_dot(_dtype_code(x), _ptr(x), _ptr(y), _ptr(s), int(n_elts),
+                                     _stream(stream)))
+
+    @staticmethod
+    def ppcg_update_scalars(alpha, beta, gamma, gammaold, delta, stream=None):
+        _check(_lib().ispm_sblas_ppcg_update_scalars(
+            _dtype_code(alpha), _ptr(alpha), _ptr(beta), _ptr(gamma), _ptr(gammaold),
+            _ptr(delta), _stream(stream)))
+
+    @staticmethod
+    def ppcg_update_vectors(resnorm, gamma, delta, alpha, beta, n, m, p, s, q, z, x, r, u, w,
+                            n_elts, stream=None):
+        _check(_lib().ispm_sblas_ppcg_update_vectors(
+            _dtype_code(x), _ptr(resnorm), _ptr(gamma), _ptr(delta), _ptr(alpha), _ptr(beta),
+            _ptr(n), _ptr(m), _ptr(p), _ptr(s), _ptr(q), _ptr(z), _ptr(x), _ptr(r), _ptr(u),
+            _ptr(w), int(n_elts), _stream(stream)))

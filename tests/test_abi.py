@@ -1,0 +1,62 @@
+"""The C-ABI library loads and exports every entry point include/*.h declares
+(no compute calls: these run without a GPU)."""
+import ctypes
+import glob
+import os
+import re
+
+from conftest import PKG, ROOT
+
+
+def declared_symbols():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"\b(ispm_[a-z0-9_]+)\s*\(", text):
+            names.add(m.group(1))
+    return names
+
+
+def test_headers_declare_entry_points():
+    names = declared_symbols()
+    assert len(names) > 40
+    assert "ispm_launch_spmv" in names and "ispm_fastainv_sym" in names
+
+
+def test_library_exports_all_declared_symbols(ispm):
+    lib = ctypes.CDLL(os.path.join(PKG, "libispm_b200.so"))
+    missing = [n for n in sorted(declared_symbols()) if not hasattr(lib, n)]
+    assert not missing, f"not exported: {missing}"
+
+
+def test_error_strings_and_version(ispm):
+    L = ispm.lib_handle()
+    assert L.ispm_error_string(0) == b"ok"
+    assert L.ispm_error_string(1) == b"invalid argument"
+    assert b"sm_100a" in L.ispm_version()
+
+
+def test_launch_params_valid_matches_reference_macro(ispm):
+    # SPMV_PARAMS_VALID_P(N, S, H) = N >= S / H && S >= H (kernel-iface.h:4)
+    for N in (64, 128, 256, 512):
+        for S in (16, 32, 64, 128, 256, 512, 1024):
+            for H in (1, 2):
+                p = ispm.spmv_launch_params(N, S, H, 1, 1)
+                assert p.valid() == (N >= S // H and S >= H)
+
+
+def test_invalid_arguments_raise(ispm, gen):
+    A = gen.poisson7(4)
+    import pytest
+    with pytest.raises(ispm.IspmError) as e:
+        ispm.csr_to_slell(A, 48, 1, False, False)  # not a power of two
+    assert e.value.status == ispm.ERR_INVALID
+    with pytest.raises(ispm.IspmError):
+        ispm.csr_to_slell(A, 32, 3, False, False)  # hblock 3
+    bad = ispm.csr_matrix(A.n_rows, A.n_cols, A.row_ptr, A.cols.copy(), A.elms)
+    bad.cols[5] = A.n_cols + 7
+    with pytest.raises(ispm.IspmError):
+        ispm.csr_to_slell(bad, 32, 1, False, True)
+    with pytest.raises(ispm.IspmError):
+        ispm.fastainv_sym(ispm.csr_matrix(0, 0, [0], [], []))
