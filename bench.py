@@ -1,0 +1,375 @@
+#!/usr/bin/env python
+"""PCG time-to-1e-10 residual on the 128^3 27-point variable-coefficient
+system, one B200 per process.
+
+Workload (synthetic, seeded): 128^3 grid, 27-point stencil, couplings
+exp((g_i + g_j)/2) / d^2 with g a Gaussian random field (correlation length 8
+cells, sigma 1.5, seed 0), diagonal = row sum + 1e-3 (SPD M-matrix; 2,097,152
+rows, 55,742,968 non-zeros).  b = A x_true with x_true ~ U(-1, 1) (seed 0).
+FSAI preconditioner from fastainv_sym with droptol 0.01 (built once, outside
+the timed region, like a time-stepping solver reuses it across solves).
+
+One step = one solve of A x = b from x = 0 until ||b - A x||_2 / ||b||_2 <=
+1e-10 (checked in FP64 with the FP64 matrix), with the mixed-precision
+pipelined PCG (FP32 SpMV and FSAI apply, FP64 reductions, FP64 refinement).
+The plain FP64 FSAI-PCG solve on the same GPU is timed beside it.
+
+The matrix (>= 226 MB per SpMV in FP32) is larger than the 126 MB L2, so no
+flush is needed between steps.  Multi-GPU: every rank solves its own copy
+(replicas; the single system is not partitioned), time = max over ranks.
+
+  python bench.py [--steps K] [--warmup W] [--gpus N] [--impl ours|reference]
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [os.path.join(ROOT, "ispm-sparse-lib_b200"), os.path.join(ROOT, "oracle")]
+
+METRIC = "PCG time-to-1e-10 residual (learned+mixed vs plain FSAI, same GPU); SpMV GB/s"
+WORKLOAD = "128^3 27-point variable-coefficient diffusion (GRF corr 8, sigma 1.5), FSAI droptol 0.01"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--grid", type=int, default=128)
+    p.add_argument("--droptol", type=float, default=0.01)
+    p.add_argument("--tol", type=float, default=1e-10)
+    p.add_argument("--cpu-sample-iters", type=int, default=20)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi sampling during the timed region (clock, throttle reasons)."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9 and f[1].isdigit():
+                    rows.append(f)
+        finally:
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [int(r[1]) for r in rows]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for name, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": int(rows[0][2]),
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# ---------------------------------------------------------------- workload
+def build_problem(ispm, gen, oracle_mod, L):
+    t0 = time.time()
+    A = gen.stencil_grf(L, 27, 8.0, 1.5, 0)
+    x_true = np.random.default_rng(0).uniform(-1, 1, A.n_rows)
+    b = oracle_spmv(A, x_true)
+    log(f"[setup] matrix {A.n_rows} rows {A.n_nz} nnz in {time.time() - t0:.1f}s")
+    return A, b
+
+
+def oracle_spmv(A, x):
+    # scipy is a plain host CSR product here: b = A x_true is input preparation
+    return A.to_scipy() @ x
+
+
+def algorithmic_bytes(view, vec_bytes):
+    """4|slice_ptr| + 4 (explicit column indices) + sizeof(E) nnz + sizeof(T)(n_cols + n_rows)."""
+    esz = 4 if view.elm_dtype == 0 else 8
+    return (4 * view.n_slice_ptr + 4 * view.n_cols_arr + esz * view.n_nz +
+            vec_bytes * (view.n_cols + view.n_rows))
+
+
+def measured_peak():
+    try:
+        m = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(m["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per launch of the A-SpMV from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "spmv_c2_fp32_diag.txt")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch:"):
+                return int(float(line.split(":")[1]))
+    except OSError:
+        pass
+    return None
+
+
+def cpu_baseline(oracle_mod, A, b, G1, G2, iters_needed, sample_iters):
+    """CPU port of the pipelined FP64 FSAI-PCG (OpenMP over the host cores):
+    time a bounded sample of iterations and scale to the iteration count the
+    full solve needs."""
+    Ac = (A.row_ptr, A.cols, A.elms)
+    g1 = (G1.row_ptr, G1.cols, np.ascontiguousarray(G1.elms, np.float64))
+    g2 = (G2.row_ptr, G2.cols, np.ascontiguousarray(G2.elms, np.float64))
+    t0 = time.perf_counter()
+    _, it, _ = oracle_mod.pcg_f64(Ac, b, g1, g2, pipelined=True, tol=1e-30, max_it=sample_iters)
+    dt = time.perf_counter() - t0
+    per_it = dt / max(it, 1)
+    return {"value": per_it * iters_needed, "unit": "s", "cores": oracle_mod.orc().orc_num_threads(),
+            "kind": "port",
+            "sample": f"{it} pipelined FP64 FSAI-PCG iterations on the host ({dt:.1f} s, CSR "
+                      f"SpMV + FSAI apply + fused updates), scaled to {iters_needed} iterations"}
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import ispm
+    import ispm.gen as gen
+    import oracle as O
+    A, b = build_problem(ispm, gen, O, args.grid)
+    t0 = time.time()
+    if O.have_ref():
+        r1, r2, _ = O.ref_fastainv_sym(A.n_rows, A.row_ptr, A.cols, A.elms, True, 2_000_000_000,
+                                       args.droptol)
+        G1 = ispm.csr_matrix(A.n_rows, A.n_cols, *r1)
+        G2 = ispm.csr_matrix(A.n_rows, A.n_cols, *r2)
+        src = "reference fastainv.cpp (compiled in place)"
+    else:
+        G1, G2 = ispm.fastainv_sym(A, np.float64, None, 2_000_000_000, args.droptol)
+        src = "fastainv restatement"
+    log(f"[reference] FSAI ({src}) {time.time() - t0:.1f}s, nnz(G) {G1.n_nz}")
+    Ac = (A.row_ptr, A.cols, A.elms)
+    g1 = (G1.row_ptr, G1.cols, G1.elms)
+    g2 = (G2.row_ptr, G2.cols, G2.elms)
+    # warm-up: one full solve fixes the iteration count the samples scale to
+    t0 = time.perf_counter()
+    _, iters, rel = O.pcg_f64(Ac, b, g1, g2, pipelined=True, tol=args.tol, max_it=20000)
+    full = time.perf_counter() - t0
+    log(f"[reference] full CPU solve: {iters} iterations, relres {rel:.2e}, {full:.1f}s")
+    times = []
+    for k in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        _, it, _ = O.pcg_f64(Ac, b, g1, g2, pipelined=True, tol=1e-30,
+                             max_it=args.cpu_sample_iters)
+        dt = (time.perf_counter() - t0) / max(it, 1) * iters
+        if k >= args.warmup:
+            times.append(dt)
+    v = float(np.mean(times))
+    cores = O.orc().orc_num_threads()
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": WORKLOAD, "grid": args.grid,
+                                        "rows": A.n_rows, "nnz": A.n_nz, "tol": args.tol,
+                                        "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": v, "unit": "s", "cores": cores, "kind": "port",
+                         "sample": f"{args.cpu_sample_iters} iterations of the host pipelined "
+                                   f"FP64 FSAI-PCG per step, scaled to the {iters} iterations "
+                                   f"of a full host solve (measured {full:.1f}s)"},
+        "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "iterations": iters, "true_relres": rel, "full_solve_s": full,
+    }), flush=True)
+
+
+# ---------------------------------------------------------------- our arm
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    import ispm
+    import ispm.gen as gen
+    import oracle as O
+    ispm.ispm_initialize()
+    dev_name = ispm.get_device_string()
+
+    A, b = build_problem(ispm, gen, O, args.grid)
+    t0 = time.time()
+    st = {}
+    G1, G2 = ispm.fastainv_sym(A, np.float64, None, 2_000_000_000, args.droptol, stats=st)
+    t_fsai = time.time() - t0
+    log(f"[setup] fastainv {t_fsai:.1f}s nnz(G) {G1.n_nz} ({st})")
+
+    t0 = time.time()
+    mixed = ispm.PCGSolver(A, G1, G2, inner=np.float32, tol=args.tol)
+    plain = ispm.PCGSolver(A, G1, G2, inner=np.float64, tol=args.tol)
+    log(f"[setup] solvers {time.time() - t0:.1f}s")
+    n_pad = mixed.rows
+    bd = torch.zeros(n_pad, dtype=torch.float64, device="cuda")
+    bd[: A.n_rows] = torch.from_numpy(b).cuda()
+    xd = torch.zeros_like(bd)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(solver, k_steps, label):
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(k_steps)]
+        stats = []
+        barrier()
+        for e0, e1 in evs:
+            e0.record(stream)
+            stats.append(solver.solve(bd, xd, stream))
+            e1.record(stream)
+        barrier()
+        ms = [e0.elapsed_time(e1) for e0, e1 in evs]
+        for s in stats:
+            if not s["converged"]:
+                raise RuntimeError(f"{label} solve did not converge: {s}")
+        return ms, stats
+
+    for _ in range(args.warmup):
+        mixed.solve(bd, xd, stream)
+        plain.solve(bd, xd, stream)
+    with ClockSampler(local) as clocks:
+        ms_mixed, st_mixed = timed(mixed, args.steps, "mixed")
+    clk = clocks.summary()
+    ms_plain, st_plain = timed(plain, max(1, min(args.steps, 3)), "plain")
+
+    # end to end through the public API: host b in, host x out, every step
+    pin_b = torch.from_numpy(b.copy()).pin_memory()
+    pin_x = torch.zeros(A.n_rows, dtype=torch.float64).pin_memory()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        mixed.solve_host(pin_b.numpy(), stream, out=pin_x.numpy())
+    barrier()
+    e2e = (time.perf_counter() - t0) / args.steps
+
+    # true residual of the last device solve, checked on the host in FP64
+    x_host = xd[: A.n_rows].cpu().numpy()
+    relres = float(np.linalg.norm(b - oracle_spmv(A, x_host)) / np.linalg.norm(b))
+
+    # dominant kernel: the FP32 SpMV of A inside the mixed solve
+    A32 = ispm.csr_matrix(A.n_rows, A.n_cols, A.row_ptr, A.cols, A.elms.astype(np.float32))
+    B32 = ispm.csr_to_slell_guess_format(A32)
+    d32 = B32.upload()
+    p = ispm.default_launch_params(d32, np.float32)
+    xs = torch.rand(A.n_cols, dtype=torch.float32, device="cuda")
+    ys = torch.zeros(B32.n_rows, dtype=torch.float32, device="cuda")
+    reps = 50
+    for _ in range(5):
+        ispm.launch_spmv_kernel(p, d32, xs, ys, stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        ispm.launch_spmv_kernel(p, d32, xs, ys, stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_spmv = e0.elapsed_time(e1) / reps * 1e-3
+    alg = algorithmic_bytes(B32.view(), 4)
+    peak, peak_src = measured_peak()
+    achieved = alg / t_spmv / 1e9
+
+    t_mixed = float(np.mean(ms_mixed)) * 1e-3
+    t_plain = float(np.mean(ms_plain)) * 1e-3
+    if world > 1:
+        tt = torch.tensor([t_mixed, e2e, t_plain], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_mixed, e2e, t_plain = tt.tolist()
+
+    launches_per_iter = 4  # G' SpMV, H' SpMV, A SpMV, fused update
+    it_mixed = st_mixed[-1]["iterations"]
+    cycles = st_mixed[-1]["refinements"]
+    gpu_launches = args.steps * (it_mixed * launches_per_iter + cycles * 8 + 2)
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(O, A, b, G1, G2, st_plain[-1]["iterations"], args.cpu_sample_iters)
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": t_mixed, "unit": "s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_mixed * 1e3,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid": args.grid, "rows": A.n_rows,
+                       "nnz": A.n_nz, "nnz_G": G1.n_nz, "tol": args.tol,
+                       "parallelism": f"replicas x{world}", "l2": "inputs larger than L2"},
+            "plain_fp64_s": t_plain, "speedup_vs_plain_fp64": t_plain / t_mixed,
+            "iterations_mixed": it_mixed, "refinements_mixed": cycles,
+            "iterations_plain": st_plain[-1]["iterations"],
+            "true_relres": relres, "fastainv_s": t_fsai,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": profile_traffic(),
+                         "kernel": "slell_spmv_kernel<float,float,H,1,V0,D1> (A, FP32)",
+                         "launch": f"N={p.N} S={p.S} H={p.H}",
+                         "algorithmic_bytes": alg, "us_per_launch": t_spmv * 1e6,
+                         "peak_source": peak_src},
+            "clocks": clk,
+            "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": 8 * A.n_rows,
+                    "d2h_bytes_per_step": 8 * A.n_rows},
+            "gpu_launches": gpu_launches,
+            "cpu_baseline": cpu,
+            "device": dev_name,
+        }
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

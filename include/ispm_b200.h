@@ -154,6 +154,10 @@ int ispm_launch_params_valid(const ispm_launch_params *p);
 int ispm_launch_spmv(int x_dtype, const ispm_launch_params *p, const ispm_slell_view *m,
                      const void *x, void *y, void *stream);
 
+/* Launch shape the library picks for a matrix without timing anything (the
+ * DEFAULT plan's choice; plan/plan.h:74-96 uses N = 512, H = 1 there). */
+int ispm_default_launch(int x_dtype, const ispm_slell_view *m, ispm_launch_params *out);
+
 /* ---- autotuning plan (plan/plan.h:9-161) -------------------------------- */
 #define ISPM_PLAN_DEFAULT 0
 #define ISPM_PLAN_ESTIMATE 1
@@ -249,6 +253,56 @@ int ispm_csr_get_info(const ispm_csr *m, int *n_rows, int *n_cols, int *n_nz, in
 int ispm_csr_get_arrays(const ispm_csr *m, const int **row_ptr, const int **cols,
                         const void **elms);
 void ispm_csr_free(ispm_csr *m);
+
+/* ---- preconditioned pipelined CG (the loop the reference leaves to its
+ *      external solver driver, README.md:5-9, built from the primitives
+ *      above: launch_spmv_kernel, sblas::ppcg_update_*, fastainv_sym) ----- */
+
+typedef struct {
+  int inner_dtype;      /* ISPM_F64: plain FP64 solve; ISPM_F32: FP32 matrices and
+                           vectors with FP64 reductions inside FP64 refinement */
+  double tol;           /* target ||b - A x||_2 / ||b||_2, checked in FP64 */
+  int max_iters;        /* total inner iterations */
+  int max_refinements;  /* outer (true-residual) cycles */
+  int check_every;      /* iterations per CUDA-graph chunk between host checks */
+  double inner_tol_f32; /* residual reduction asked of one FP32 inner solve */
+  int use_graph;        /* replay iteration chunks as a CUDA graph */
+} ispm_solver_opts;
+
+typedef struct {
+  int iterations;       /* inner iterations over all cycles */
+  int refinements;      /* outer cycles */
+  int converged;
+  int status;
+  double true_relres;   /* ||b - A x||_2 / ||b||_2 with the FP64 matrix */
+  double seconds;       /* host wall time of the solve call */
+} ispm_solve_stats;
+
+void ispm_solver_default_opts(ispm_solver_opts *opts);
+
+typedef struct ispm_solver ispm_solver;
+
+/* A: n x n SPD CSR in FP64 (host).  (g1, g2): the fastainv_sym pair
+ * (Ainv1, Ainv2) in FP64 (host), or all NULL for no preconditioner.  The
+ * solver keeps device copies only (FP64 A for residuals, A and the factor
+ * pair in the inner type). */
+int ispm_solver_create(int n, const int *row_ptr, const int *cols, const double *vals,
+                       const int *g1_row_ptr, const int *g1_cols, const double *g1_vals,
+                       const int *g2_row_ptr, const int *g2_cols, const double *g2_vals,
+                       const ispm_solver_opts *opts, ispm_solver **out);
+/* Padded row count (the length of the device vectors the solver expects). */
+int ispm_solver_rows(const ispm_solver *s);
+/* Solve A x = b; b and x are device FP64 vectors of ispm_solver_rows()
+ * entries (x is overwritten; the solve starts from zero). */
+int ispm_solver_solve(ispm_solver *s, const double *b, double *x, ispm_solve_stats *stats,
+                      void *stream);
+/* Same with host vectors of n entries: copies b in and x out inside the call. */
+int ispm_solver_solve_host(ispm_solver *s, const double *b_host, double *x_host,
+                           ispm_solve_stats *stats, void *stream);
+/* True relative residual after each outer cycle of the last solve; returns
+ * the count (writes at most cap values). */
+int ispm_solver_history(const ispm_solver *s, double *out, int cap);
+void ispm_solver_free(ispm_solver *s);
 
 /* ---- drop-tolerance tuner (fastainv/droptol-tuning.h:4-103) ------------ */
 typedef struct ispm_droptol_tuner ispm_droptol_tuner;

@@ -209,4 +209,13 @@ int ispm_dslell_get_view(const ispm_dslell *d, ispm_slell_view *view)
 
 void ispm_dslell_free(ispm_dslell *d) { delete d; }
 
+int ispm_default_launch(int x_dtype, const ispm_slell_view *m, ispm_launch_params *out)
+{
+  clear_error();
+  if (!m || !out)
+    return fail(ISPM_ERR_INVALID, "NULL argument");
+  *out = default_launch(x_dtype, *m);
+  return check_launch(x_dtype, *out, *m);
+}
+
 }  // extern "C"

@@ -19,6 +19,8 @@
 //  * hblock columns gather W consecutive x values with one vector load.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "cuda_util.cuh"
 #include "spmv_launch.h"
 
@@ -37,6 +39,8 @@ template <class T, class E> struct SpmvArgs {
   unsigned tps;       // threads per slice (reference N), power of two
   unsigned log2_tps;
   int x_vec_ok;       // x aligned for W-wide vector loads
+  int x_al16;         // x 16-byte aligned (diagonal-window vector loads)
+  const int *skip;    // optional device flag: nonzero -> the launch does nothing
 };
 
 // Gather x[c*W .. c*W+W-1] into xw, zero beyond n_cols.
@@ -78,10 +82,54 @@ __device__ __forceinline__ void gather_w(const T *__restrict__ x, unsigned c, un
     xw[w] = ld_x_guard(x, base + w, n_cols);
 }
 
+// x[base .. base+H-1] for one diagonal, zero outside [0, n).  Within a slice
+// base = diag_pos + row - slice_height with row a multiple of H, so
+// base mod H is the same for every thread of the slice: when H values of T
+// fill 16 bytes, the window is one aligned 128-bit load (two when base is
+// not H-aligned) instead of H scalar loads that each touch the whole warp's
+// span of cache lines.
+template <class T, int H>
+__device__ __forceinline__ void load_window(const T *__restrict__ x, unsigned base, unsigned n,
+                                            bool vec_ok, T (&xv)[H])
+{
+  if constexpr (H * sizeof(T) == 16) {
+    using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+    const unsigned sh = base & (H - 1);
+    const unsigned a0 = base - sh;
+    if (vec_ok && a0 < n && n - a0 >= (sh ? 2u * H : (unsigned)H)) {
+      T w[2 * H];
+      V v0 = __ldg(reinterpret_cast<const V *>(x + a0));
+      *reinterpret_cast<V *>(w) = v0;
+      if (sh) {
+        V v1 = __ldg(reinterpret_cast<const V *>(x + a0 + H));
+        *reinterpret_cast<V *>(w + H) = v1;
+      } else {
+#pragma unroll
+        for (int k = H; k < 2 * H; k++)
+          w[k] = T(0);
+      }
+#pragma unroll
+      for (int h = 0; h < H; h++) {
+        T r = w[h];
+#pragma unroll
+        for (int k = 1; k < H; k++)
+          r = sh == (unsigned)k ? w[h + k] : r;
+        xv[h] = r;
+      }
+      return;
+    }
+  }
+#pragma unroll
+  for (int h = 0; h < H; h++)
+    xv[h] = ld_x_guard(x, base + h, n);
+}
+
 template <class T, class E, int H, int W, bool VAR, bool DIAG>
 __global__ void __launch_bounds__(1024) slell_spmv_kernel(SpmvArgs<T, E> a)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (a.skip && *a.skip)  // uniform: a converged solver's graph replays as no-ops
+    return;
   constexpr unsigned spe = 1 + (W > 1) + (VAR ? 1 : 0) + (DIAG ? 2 : 0);
   const unsigned tps = a.tps;
   const unsigned t = threadIdx.x & (tps - 1);
@@ -140,13 +188,16 @@ __global__ void __launch_bounds__(1024) slell_spmv_kernel(SpmvArgs<T, E> a)
     const unsigned adj = ((t * H) & (sz - 1)) - sz;
     unsigned jj = d0 + (j - c1) / sz;
     const unsigned jstep = step / sz;
+    const bool vec_ok = a.x_al16;
 #pragma unroll 4
     for (; i < e1; i += step, jj += jstep) {
       const unsigned base = __ldg(a.sp + jj) + adj;
       Vec<H, E> ee = ld_stream<H>(a.elms + i);
+      T xv[H];
+      load_window<T, H>(a.x, base, a.n_cols, vec_ok, xv);
 #pragma unroll
       for (int h = 0; h < H; h++)
-        acc[h] = fma(T(ee.v[h]), ld_x_guard(a.x, base + h, a.n_cols), acc[h]);
+        acc[h] = fma(T(ee.v[h]), xv[h], acc[h]);
     }
   } else if constexpr (W > 1) {
     // hblock columns (kernel.h:93-119): W values per stored column index.
@@ -241,9 +292,10 @@ int launch_h(const SpmvArgs<T, E> &args, const ispm_slell_view &m, unsigned tps,
 
 template <class T, class E>
 int launch_te(const ispm_launch_params &p, const ispm_slell_view &m, const void *x, void *y,
-              cudaStream_t s)
+              cudaStream_t s, const int *skip)
 {
   SpmvArgs<T, E> a;
+  a.skip = skip;
   a.sp = m.slice_ptr;
   a.cols = m.cols;
   a.elms = static_cast<const E *>(m.elms);
@@ -255,6 +307,7 @@ int launch_te(const ispm_launch_params &p, const ispm_slell_view &m, const void 
   a.tps = p.N;
   a.log2_tps = (unsigned)ilog2(p.N);
   a.x_vec_ok = aligned(x, (size_t)m.hblock * sizeof(T));
+  a.x_al16 = aligned(x, 16);
   if (!aligned(m.elms, p.H * sizeof(E)) || !aligned(m.cols, p.H * sizeof(unsigned)) ||
       !aligned(y, p.H * sizeof(T)))
     return fail(ISPM_ERR_INVALID, "matrix arrays or y not aligned to H=%u elements", p.H);
@@ -307,7 +360,7 @@ int check_launch(int x_dtype, const ispm_launch_params &p, const ispm_slell_view
 }
 
 int launch_spmv(int x_dtype, const ispm_launch_params &p, const ispm_slell_view &m,
-                const void *x, void *y, cudaStream_t s)
+                const void *x, void *y, cudaStream_t s, const int *skip)
 {
   int st = check_launch(x_dtype, p, m);
   if (st || m.n_slices == 0)
@@ -315,10 +368,10 @@ int launch_spmv(int x_dtype, const ispm_launch_params &p, const ispm_slell_view 
   if (!x || !y || !m.slice_ptr || (m.n_elms && (!m.elms)) || (m.n_cols_arr && !m.cols))
     return fail(ISPM_ERR_INVALID, "NULL pointer");
   if (x_dtype == ISPM_F32)
-    return launch_te<float, float>(p, m, x, y, s);
+    return launch_te<float, float>(p, m, x, y, s, skip);
   if (m.elm_dtype == ISPM_F32)
-    return launch_te<double, float>(p, m, x, y, s);
-  return launch_te<double, double>(p, m, x, y, s);
+    return launch_te<double, float>(p, m, x, y, s, skip);
+  return launch_te<double, double>(p, m, x, y, s, skip);
 }
 
 }  // namespace ispm

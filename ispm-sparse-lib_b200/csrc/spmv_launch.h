@@ -10,9 +10,10 @@ namespace ispm {
 
 // Validate launch parameters against a matrix (no CUDA calls).
 int check_launch(int x_dtype, const ispm_launch_params &p, const ispm_slell_view &m);
-// Validate and launch y = A x on `s`.
+// Validate and launch y = A x on `s`.  `skip` (device int, may be NULL): the
+// kernel returns at once when it holds a nonzero value.
 int launch_spmv(int x_dtype, const ispm_launch_params &p, const ispm_slell_view &m,
-                const void *x, void *y, cudaStream_t s);
+                const void *x, void *y, cudaStream_t s, const int *skip = nullptr);
 
 // Device-resident sliced-ELL matrix.
 struct DeviceSlell {

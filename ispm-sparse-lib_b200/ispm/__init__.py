@@ -558,3 +558,137 @@ class sblas:
             _dtype_code(x), _ptr(resnorm), _ptr(gamma), _ptr(delta), _ptr(alpha), _ptr(beta),
             _ptr(n), _ptr(m), _ptr(p), _ptr(s), _ptr(q), _ptr(z), _ptr(x), _ptr(r), _ptr(u),
             _ptr(w), int(n_elts), _stream(stream)))
+
+
+# ---------------------------------------------------------------------------
+# Pipelined PCG with FP64 refinement (the loop of the reference's external
+# solver driver, composed from the primitives above)
+# ---------------------------------------------------------------------------
+
+class solver_opts(C.Structure):
+    _fields_ = [("inner_dtype", C.c_int), ("tol", C.c_double), ("max_iters", C.c_int),
+                ("max_refinements", C.c_int), ("check_every", C.c_int),
+                ("inner_tol_f32", C.c_double), ("use_graph", C.c_int)]
+
+
+class solve_stats(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("refinements", C.c_int), ("converged", C.c_int),
+                ("status", C.c_int), ("true_relres", C.c_double), ("seconds", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_SOLVER_DECLARED = False
+
+
+def _declare_solver():
+    global _SOLVER_DECLARED
+    if _SOLVER_DECLARED:
+        return
+    L = _lib()
+    vp, i = C.c_void_p, C.c_int
+    L.ispm_solver_default_opts.argtypes = [C.POINTER(solver_opts)]
+    L.ispm_solver_default_opts.restype = None
+    L.ispm_solver_create.argtypes = [i, vp, vp, vp, vp, vp, vp, vp, vp, vp,
+                                     C.POINTER(solver_opts), C.POINTER(vp)]
+    L.ispm_solver_create.restype = i
+    L.ispm_solver_rows.argtypes = [vp]
+    L.ispm_solver_rows.restype = i
+    L.ispm_solver_solve.argtypes = [vp, vp, vp, C.POINTER(solve_stats), vp]
+    L.ispm_solver_solve.restype = i
+    L.ispm_solver_solve_host.argtypes = [vp, vp, vp, C.POINTER(solve_stats), vp]
+    L.ispm_solver_solve_host.restype = i
+    L.ispm_solver_history.argtypes = [vp, vp, i]
+    L.ispm_solver_history.restype = i
+    L.ispm_solver_free.argtypes = [vp]
+    L.ispm_solver_free.restype = None
+    _SOLVER_DECLARED = True
+
+
+class PCGSolver:
+    """Preconditioned pipelined CG with FP64 iterative refinement.
+
+    A: FP64 csr_matrix (SPD).  G1, G2: the fastainv_sym pair (Ainv1, Ainv2) or
+    None.  inner: np.float64 (plain FP64) or np.float32 (mixed precision: FP32
+    matrices / vectors, FP64 reductions, FP64 outer residual)."""
+
+    def __init__(self, A: csr_matrix, G1: csr_matrix | None = None,
+                 G2: csr_matrix | None = None, inner=np.float32, tol: float = 1e-10,
+                 max_iters: int = 100000, max_refinements: int = 50, check_every: int = 16,
+                 inner_tol_f32: float = 1e-5, use_graph: bool = True):
+        _declare_solver()
+        L = _lib()
+        o = solver_opts()
+        L.ispm_solver_default_opts(C.byref(o))
+        o.inner_dtype = F64 if np.dtype(inner) == np.float64 else F32
+        o.tol, o.max_iters, o.max_refinements = tol, max_iters, max_refinements
+        o.check_every, o.inner_tol_f32, o.use_graph = check_every, inner_tol_f32, int(use_graph)
+        if A.elms.dtype != np.float64:
+            raise TypeError("the solver takes the FP64 matrix")
+        self._keep = [A, G1, G2]
+        out = C.c_void_p()
+        G1e = None if G1 is None else np.ascontiguousarray(G1.elms, np.float64)
+        G2e = None if G2 is None else np.ascontiguousarray(G2.elms, np.float64)
+        self._keep += [G1e, G2e]
+        args = [A.n_rows, _ptr(A.row_ptr), _ptr(A.cols), _ptr(A.elms),
+                None if G1 is None else _ptr(G1.row_ptr), None if G1 is None else _ptr(G1.cols),
+                None if G1 is None else _ptr(G1e),
+                None if G2 is None else _ptr(G2.row_ptr), None if G2 is None else _ptr(G2.cols),
+                None if G2 is None else _ptr(G2e)]
+        _check(L.ispm_solver_create(*args, C.byref(o), C.byref(out)))
+        self._h = out
+        self.n = A.n_rows
+        self.opts = o
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _L is not None:
+            _L.ispm_solver_free(self._h)
+            self._h = None
+
+    @property
+    def rows(self) -> int:
+        return int(_lib().ispm_solver_rows(self._h))
+
+    def _finish(self, status, st):
+        if status not in (OK, ERR_NOT_CONVERGED, ERR_BREAKDOWN):
+            _check(status)
+        return st.as_dict()
+
+    def solve(self, b, x, stream=None) -> dict:
+        """b, x: FP64 device vectors of `rows` entries (torch tensors or pointers)."""
+        st = solve_stats()
+        rc = _lib().ispm_solver_solve(self._h, _ptr(b), _ptr(x), C.byref(st), _stream(stream))
+        return self._finish(rc, st)
+
+    def solve_host(self, b: np.ndarray, stream=None, out: np.ndarray | None = None):
+        """Host vectors: copies b in and x out inside the call (into `out` when
+        given, e.g. a pinned buffer).  Returns (x, stats)."""
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros(self.n) if out is None else out
+        assert x.dtype == np.float64 and x.flags.c_contiguous and x.size >= self.n
+        st = solve_stats()
+        rc = _lib().ispm_solver_solve_host(self._h, _ptr(b), _ptr(x), C.byref(st),
+                                           _stream(stream))
+        return x, self._finish(rc, st)
+
+    def history(self):
+        buf = np.zeros(256)
+        k = _lib().ispm_solver_history(self._h, _ptr(buf), 256)
+        return buf[: min(k, 256)].copy()
+
+
+def default_launch_params(m, x_dtype=None) -> spmv_launch_params:
+    """The launch shape the DEFAULT plan uses for matrix m (host or device)."""
+    L = _lib()
+    L.ispm_default_launch.argtypes = [C.c_int, C.POINTER(slell_view),
+                                      C.POINTER(spmv_launch_params)]
+    L.ispm_default_launch.restype = C.c_int
+    v = m.view()
+    if x_dtype is None:
+        x_dtype = v.elm_dtype
+    elif not isinstance(x_dtype, int):
+        x_dtype = F64 if np.dtype(x_dtype) == np.float64 else F32
+    p = spmv_launch_params()
+    _check(L.ispm_default_launch(int(x_dtype), C.byref(v), C.byref(p)))
+    return p

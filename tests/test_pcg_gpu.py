@@ -1,0 +1,94 @@
+"""Pipelined PCG on the GPU: every solve is judged by its true residual
+||b - A x||_2 / ||b||_2 computed on the CPU with the FP64 CSR oracle; the
+iteration counts of the FP64 path track the CPU oracle's pipelined PCG (the
+sblas.cu:156-216 recurrences in FP64) on the same FSAI preconditioner."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def c1(ispm, gen, oracle):
+    """Config 1: 32^3 7-point Poisson, x_true ~ U(-1, 1) seed 0, b = A x_true,
+    FSAI droptol 0.01."""
+    A = gen.poisson7(32)
+    x_true = np.random.default_rng(0).uniform(-1, 1, A.n_rows)
+    b = oracle.csr_spmv_f64(A.row_ptr, A.cols, A.elms, x_true)
+    G1, G2 = ispm.fastainv_sym(A, np.float64, None, 8192000, 0.01)
+    return A, b, G1, G2
+
+
+def true_relres(oracle, A, b, x):
+    r = b - oracle.csr_spmv_f64(A.row_ptr, A.cols, A.elms, x)
+    return np.linalg.norm(r) / np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("inner", [np.float64, np.float32], ids=["fp64", "mixed"])
+@pytest.mark.parametrize("tol", [1e-8, 1e-10])
+def test_pcg_c1_true_residual(ispm, oracle, cuda, c1, inner, tol):
+    A, b, G1, G2 = c1
+    s = ispm.PCGSolver(A, G1, G2, inner=inner, tol=tol)
+    x, st = s.solve_host(b)
+    assert st["converged"] and st["status"] == 0, st
+    rel = true_relres(oracle, A, b, x)
+    assert rel <= tol * 1.001, (rel, st)
+    assert abs(rel - st["true_relres"]) <= 0.05 * rel + 1e-16  # GPU FP64 residual agrees
+    if inner == np.float64:
+        _, it_cpu, _ = oracle.pcg_f64((A.row_ptr, A.cols, A.elms), b,
+                                      (G1.row_ptr, G1.cols, G1.elms),
+                                      (G2.row_ptr, G2.cols, G2.elms), pipelined=True, tol=tol)
+        assert abs(st["iterations"] - it_cpu) <= max(3, 0.05 * it_cpu), (st, it_cpu)
+
+
+def test_pcg_device_vectors_graph_and_eager_agree(ispm, oracle, cuda, c1):
+    A, b, G1, G2 = c1
+    outs = []
+    for use_graph in (True, False):
+        s = ispm.PCGSolver(A, G1, G2, inner=np.float32, tol=1e-10, use_graph=use_graph)
+        bd = cuda.zeros(s.rows, dtype=cuda.float64, device="cuda")
+        bd[: A.n_rows] = cuda.from_numpy(b).cuda()
+        xd = cuda.zeros_like(bd)
+        st = s.solve(bd, xd)
+        assert st["converged"]
+        outs.append((xd.cpu().numpy(), st))
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert outs[0][1]["iterations"] == outs[1][1]["iterations"]
+    assert true_relres(oracle, A, b, outs[0][0][: A.n_rows]) <= 1e-10
+
+
+def test_pcg_without_preconditioner_and_grf(ispm, oracle, cuda, gen):
+    A = gen.stencil_grf(16, 27, 4.0, 1.5, 3)
+    x_true = np.random.default_rng(1).uniform(-1, 1, A.n_rows)
+    b = oracle.csr_spmv_f64(A.row_ptr, A.cols, A.elms, x_true)
+    for inner in (np.float64, np.float32):
+        s = ispm.PCGSolver(A, None, None, inner=inner, tol=1e-9)
+        x, st = s.solve_host(b)
+        assert st["converged"], st
+        assert true_relres(oracle, A, b, x) <= 1e-9 * 1.001
+    G1, G2 = ispm.fastainv_sym(A, np.float64, None, 50_000_000, 0.01)
+    s = ispm.PCGSolver(A, G1, G2, inner=np.float32, tol=1e-10)
+    x, st = s.solve_host(b)
+    assert st["converged"] and true_relres(oracle, A, b, x) <= 1e-10 * 1.001
+
+
+def test_pcg_zero_rhs_and_limits(ispm, oracle, cuda, c1):
+    A, b, G1, G2 = c1
+    s = ispm.PCGSolver(A, G1, G2, inner=np.float64, tol=1e-10)
+    x, st = s.solve_host(np.zeros_like(b))
+    assert st["converged"] and np.all(x == 0)
+    s2 = ispm.PCGSolver(A, G1, G2, inner=np.float64, tol=1e-14, max_iters=5)
+    x, st = s2.solve_host(b)
+    assert not st["converged"] and st["status"] == ispm.ERR_NOT_CONVERGED
+    assert st["iterations"] <= 5 + 16
+
+
+def test_pcg_indefinite_matrix_stops(ispm, cuda):
+    # symmetric indefinite: CG breaks down; the solver must stop and report it
+    n = 64
+    d = np.where(np.arange(n) % 2 == 0, 2.0, -2.0)
+    rp = np.arange(n + 1, dtype=np.int32)
+    A = ispm.csr_matrix(n, n, rp, np.arange(n, dtype=np.int32), d)
+    s = ispm.PCGSolver(A, None, None, inner=np.float64, tol=1e-10, max_refinements=3)
+    x, st = s.solve_host(np.ones(n))
+    assert not st["converged"] or np.allclose(x, 1.0 / d)
