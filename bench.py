@@ -49,7 +49,34 @@ def parse():
     p.add_argument("--tol", type=float, default=1e-10)
     p.add_argument("--cpu-sample-iters", type=int, default=20)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--kernel-only", choices=["spmv32", "spmv64"], default=None,
+                   help="only launch the A SpMV of the workload (FP32 or FP64) --reps times "
+                        "(a small program for ncu captures)")
+    p.add_argument("--reps", type=int, default=5)
     return p.parse_args()
+
+
+def kernel_only(args):
+    """Upload the workload matrix in the guessed format and launch its SpMV
+    --reps times with the DEFAULT plan's launch shape."""
+    import torch
+    import ispm
+    import ispm.gen as gen
+    ispm.ispm_initialize()
+    A = gen.stencil_grf(args.grid, 27, 8.0, 1.5, 0)
+    dt = np.float32 if args.kernel_only == "spmv32" else np.float64
+    Ae = ispm.csr_matrix(A.n_rows, A.n_cols, A.row_ptr, A.cols, A.elms.astype(dt))
+    B = ispm.csr_to_slell_guess_format(Ae)
+    d = B.upload()
+    del B
+    p = ispm.default_launch_params(d, dt)
+    tdt = torch.float32 if dt == np.float32 else torch.float64
+    x = torch.rand(A.n_cols, dtype=tdt, device="cuda")
+    y = torch.zeros(d.n_rows, dtype=tdt, device="cuda")
+    for _ in range(args.reps):
+        ispm.launch_spmv_kernel(p, d, x, y)
+    torch.cuda.synchronize()
+    log(f"[kernel-only] {args.kernel_only} {p} x{args.reps} done")
 
 
 def log(*a):
@@ -174,17 +201,17 @@ def run_reference(args, rank, world):
     import ispm
     import ispm.gen as gen
     import oracle as O
+    if not O.have_ref():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference's "
+                          "fastainv.cpp compiled in place) was not built on this machine"}))
+        return
     A, b = build_problem(ispm, gen, O, args.grid)
     t0 = time.time()
-    if O.have_ref():
-        r1, r2, _ = O.ref_fastainv_sym(A.n_rows, A.row_ptr, A.cols, A.elms, True, 2_000_000_000,
-                                       args.droptol)
-        G1 = ispm.csr_matrix(A.n_rows, A.n_cols, *r1)
-        G2 = ispm.csr_matrix(A.n_rows, A.n_cols, *r2)
-        src = "reference fastainv.cpp (compiled in place)"
-    else:
-        G1, G2 = ispm.fastainv_sym(A, np.float64, None, 2_000_000_000, args.droptol)
-        src = "fastainv restatement"
+    r1, r2, _ = O.ref_fastainv_sym(A.n_rows, A.row_ptr, A.cols, A.elms, True, 2_000_000_000,
+                                   args.droptol)
+    G1 = ispm.csr_matrix(A.n_rows, A.n_cols, *r1)
+    G2 = ispm.csr_matrix(A.n_rows, A.n_cols, *r2)
+    src = "reference fastainv.cpp (compiled in place)"
     log(f"[reference] FSAI ({src}) {time.time() - t0:.1f}s, nnz(G) {G1.n_nz}")
     Ac = (A.row_ptr, A.cols, A.elms)
     g1 = (G1.row_ptr, G1.cols, G1.elms)
@@ -228,6 +255,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.kernel_only:
+        return kernel_only(args)
 
     import torch
     import torch.distributed as dist
@@ -331,10 +360,13 @@ def main():
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         t_mixed, e2e, t_plain = tt.tolist()
 
-    launches_per_iter = 4  # G' SpMV, H' SpMV, A SpMV, fused update
+    # classic FP32 iteration: A SpMV (+p.Ap), r/x update, G' SpMV, H' SpMV (+r.z),
+    # new direction; each reliable update: fold, FP64 SpMV, residual, load, G',
+    # H', direction
+    launches_per_iter = 5
     it_mixed = st_mixed[-1]["iterations"]
     cycles = st_mixed[-1]["refinements"]
-    gpu_launches = args.steps * (it_mixed * launches_per_iter + cycles * 8 + 2)
+    gpu_launches = args.steps * (it_mixed * launches_per_iter + (cycles + 1) * 7 + 2)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:

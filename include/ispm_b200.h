@@ -260,18 +260,26 @@ void ispm_csr_free(ispm_csr *m);
 
 typedef struct {
   int inner_dtype;      /* ISPM_F64: plain FP64 solve; ISPM_F32: FP32 matrices and
-                           vectors with FP64 reductions inside FP64 refinement */
+                           vectors, FP64 reductions and FP64 reliable updates */
   double tol;           /* target ||b - A x||_2 / ||b||_2, checked in FP64 */
-  int max_iters;        /* total inner iterations */
-  int max_refinements;  /* outer (true-residual) cycles */
+  int max_iters;        /* total iterations */
+  int max_refinements;  /* reliable updates + restarts */
   int check_every;      /* iterations per CUDA-graph chunk between host checks */
-  double inner_tol_f32; /* residual reduction asked of one FP32 inner solve */
   int use_graph;        /* replay iteration chunks as a CUDA graph */
+  double replace_ratio_f32; /* reliable update once the recursive residual fell by
+                               this factor since the last one (FP32 inner) */
+  double replace_ratio_f64; /* same for FP64 */
+  int variant;          /* ISPM_PCG_AUTO (pipelined in FP64, classic in FP32),
+                           ISPM_PCG_PIPELINED or ISPM_PCG_CLASSIC */
 } ispm_solver_opts;
 
+#define ISPM_PCG_AUTO 0
+#define ISPM_PCG_PIPELINED 1
+#define ISPM_PCG_CLASSIC 2
+
 typedef struct {
-  int iterations;       /* inner iterations over all cycles */
-  int refinements;      /* outer cycles */
+  int iterations;       /* iterations over the whole solve */
+  int refinements;      /* reliable updates (true-residual replacements) + restarts */
   int converged;
   int status;
   double true_relres;   /* ||b - A x||_2 / ||b||_2 with the FP64 matrix */

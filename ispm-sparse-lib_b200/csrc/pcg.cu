@@ -1,5 +1,5 @@
-// Preconditioned pipelined CG on sliced-ELL operands, with FP64 iterative
-// refinement.
+// Preconditioned pipelined CG on sliced-ELL operands with FP64 reliable
+// updates.
 //
 // The reference ships the primitives of this loop -- SpMV
 // (cuda/spmv/kernel-iface.h), ppcg_update_scalars / ppcg_update_vectors
@@ -10,13 +10,19 @@
 //    update kernel that also derives alpha / beta on the device, so an
 //    iteration never waits on the host; chunks of iterations are captured in
 //    a CUDA graph and replayed, and a device "done" flag turns the rest of a
-//    chunk into no-ops once the recursive residual meets the target;
+//    chunk into no-ops as soon as the solve needs the host;
 //  * reductions (gamma = r.u, delta = w.u, ||r||^2) accumulate in FP64 and
 //    finish in the last CTA of the update launch;
 //  * inner precision T is FP64 (plain) or FP32 (mixed: FP32 matrices and
-//    vectors, FP64 reductions); an FP64 outer loop recomputes the true
-//    residual b - A x with the FP64 matrix and restarts the inner solve on it
-//    until ||b - A x||_2 <= tol ||b||_2;
+//    vectors, FP64 reductions);
+//  * reliable updates (residual replacement): whenever the recursive residual
+//    has dropped by `replace_ratio` since the last update, or meets the
+//    target, the correction accumulated in T is folded into the FP64 iterate,
+//    r = b - A x is recomputed with the FP64 matrix, and the pipelined
+//    auxiliaries are re-derived from it (u = M r, w = A u, s = A p, q = M s,
+//    z = A q) without restarting the Krylov recurrence.  This bounds the
+//    drift between the recursive and the true residual that otherwise stalls
+//    pipelined CG in FP32 (and limits its attainable accuracy in FP64);
 //  * the FSAI pair is stored as G' = P Ainv1 (rows reversed) and H' = Ainv2 P
 //    (columns reversed), P the index reversal: M = Ainv2 Ainv1 = H' G', and
 //    both factors become banded with stencil-like diagonals that the
@@ -26,6 +32,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -40,22 +48,27 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kMaxBlocks = 1024;
 
+enum Done { kRunning = 0, kConverged = 1, kBreakdown = 2, kCap = 3, kReplace = 4 };
+
 // Device-resident solver scalars.
 struct PcgState {
   double gamma, gammaold, delta, alpha, beta;
-  double rr;       // ||r||^2 of the inner recursive residual
-  double rr0;      // ||r||^2 when the inner solve started
-  double thresh2;  // inner stop: rr <= thresh2
-  double res2;     // ||b - A x||^2 of the last outer residual
-  double rscale;   // norm the inner right-hand side was divided by
-  int it;          // inner iterations so far
-  int max_it;      // inner iteration cap
-  int done;        // 0 running, 1 converged, 2 breakdown, 3 iteration cap
-  int pad;
+  double rr;       // ||r||^2 of the recursive residual
+  double rr_ref;   // ||r||^2 at the last reliable update
+  double thresh2;  // recursive residual target (absolute, squared)
+  double ru2;      // replacement trigger: rr < ru2 * rr_ref
+  double res2;     // ||b - A x||^2 of the last true residual
+  double pq;       // classic CG: p.Ap
+  double rz;       // classic CG: r.z of the current direction
+  double rz_new;   // classic CG: r.z of the updated residual
+  int it;          // iterations since the last full restart
+  int max_it;      // iteration cap for this restart
+  int done;        // Done
+  int fresh;       // classic CG: next direction update starts a new sequence
 };
 
 struct Scratch {
-  double *part;     // 4 * kMaxBlocks partials
+  double *part;  // 4 * kMaxBlocks partials
   unsigned *ticket;
 };
 
@@ -123,10 +136,23 @@ template <int NV> __device__ bool grid_total(Acc<NV> a, Scratch sc, Acc<NV> &tot
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (n); \
        i += (long long)gridDim.x * blockDim.x)
 
+// x += d (FP64 iterate, correction in T), d = 0; then r64 = b - A x needs the
+// SpMV, done separately.
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+    fold_correction_kernel(double *__restrict__ x, T *__restrict__ d, long long n)
+{
+  GRID_STRIDE(i, n)
+  {
+    x[i] += (double)d[i];
+    d[i] = T(0);
+  }
+}
+
 // r64 = b - Ax, res2 = ||r64||^2
 __global__ void __launch_bounds__(kThreads)
-    outer_residual_kernel(const double *__restrict__ b, const double *__restrict__ ax,
-                          double *__restrict__ r, long long n, PcgState *st, Scratch sc)
+    true_residual_kernel(const double *__restrict__ b, const double *__restrict__ ax,
+                         double *__restrict__ r, long long n, PcgState *st, Scratch sc)
 {
   Acc<1> a{{0.0}};
   GRID_STRIDE(i, n)
@@ -140,34 +166,33 @@ __global__ void __launch_bounds__(kThreads)
     st->res2 = tot.v[0];
 }
 
-// Inner right-hand side r = r64 / ||r64|| in T; zero the inner iterate and
-// the recurrence vectors.
+// r = (T) r64 on the real rows (0 on padding); on a full restart also zero
+// the search-direction recurrences.
 template <class T>
 __global__ void __launch_bounds__(kThreads)
-    scale_rhs_kernel(const double *__restrict__ r64, T *r, T *d, T *p, T *s, T *q, T *z,
-                     long long n, long long n_pad, PcgState *st)
+    load_residual_kernel(const double *__restrict__ r64, T *r, T *d, T *p, T *s, T *q, T *z,
+                         long long n, long long n_pad, int restart)
 {
-  const double nrm = sqrt(st->res2);
-  const double inv = nrm > 0 ? 1.0 / nrm : 0.0;
   GRID_STRIDE(i, n_pad)
   {
-    r[i] = i < n ? (T)(r64[i] * inv) : T(0);
+    r[i] = i < n ? (T)r64[i] : T(0);
     d[i] = T(0);
-    p[i] = T(0);
-    s[i] = T(0);
-    q[i] = T(0);
-    z[i] = T(0);
+    if (restart) {
+      p[i] = T(0);
+      s[i] = T(0);
+      q[i] = T(0);
+      z[i] = T(0);
+    }
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0)
-    st->rscale = nrm;
 }
 
-// gamma = r.u, delta = w.u, rr = r.r at the start of an inner solve.
+// gamma = r.u, delta = w.u, rr = r.r after a (re)start; keeps the previous
+// alpha / gamma on a replacement so the recurrence continues.
 template <class T>
 __global__ void __launch_bounds__(kThreads)
-    init_dots_kernel(const T *__restrict__ r, const T *__restrict__ u,
-                     const T *__restrict__ w, long long n, PcgState *st, Scratch sc,
-                     double rel_tol, int max_it)
+    sync_dots_kernel(const T *__restrict__ r, const T *__restrict__ u, const T *__restrict__ w,
+                     long long n, PcgState *st, Scratch sc, double thresh2, double ru2,
+                     int max_it, int restart)
 {
   Acc<3> a{{0.0, 0.0, 0.0}};
   GRID_STRIDE(i, n)
@@ -182,14 +207,17 @@ __global__ void __launch_bounds__(kThreads)
     st->gamma = tot.v[0];
     st->delta = tot.v[1];
     st->rr = tot.v[2];
-    st->rr0 = tot.v[2];
-    st->thresh2 = rel_tol * rel_tol * tot.v[2];
-    st->gammaold = 0;
-    st->alpha = 0;
-    st->beta = 0;
-    st->it = 0;
+    st->rr_ref = tot.v[2];
+    st->thresh2 = thresh2;
+    st->ru2 = ru2;
+    if (restart) {
+      st->gammaold = 0;
+      st->alpha = 0;
+      st->beta = 0;
+      st->it = 0;
+    }
     st->max_it = max_it;
-    st->done = tot.v[2] == 0.0 ? 1 : 0;
+    st->done = tot.v[2] <= thresh2 ? kConverged : kRunning;
   }
 }
 
@@ -215,10 +243,10 @@ __global__ void __launch_bounds__(kThreads)
     alpha = g / (de - beta * g / st->alpha);
   }
   if (!(alpha > 0.0) || !isfinite(alpha) || !isfinite(beta)) {
-    // Lost positive definiteness in finite precision: stop, the outer loop
-    // restarts from the true residual.
+    // Lost positive definiteness in finite precision: stop; the host folds
+    // the correction in and restarts from the true residual.
     if (blockIdx.x == 0 && threadIdx.x == 0)
-      st->done = 2;
+      st->done = kBreakdown;
     return;
   }
   const T a = (T)alpha, b = (T)beta;
@@ -254,21 +282,128 @@ __global__ void __launch_bounds__(kThreads)
     st->delta = tot.v[1];
     st->rr = tot.v[2];
     st->it += 1;
-    if (!(tot.v[2] > st->thresh2))
-      st->done = isfinite(tot.v[2]) ? 1 : 2;
+    if (!isfinite(tot.v[2]) || !isfinite(tot.v[0]))
+      st->done = kBreakdown;
+    else if (tot.v[2] <= st->thresh2)
+      st->done = kConverged;
+    else if (tot.v[2] < st->ru2 * st->rr_ref)
+      st->done = kReplace;
     else if (st->it >= st->max_it)
-      st->done = 3;
+      st->done = kCap;
   }
 }
 
-// x += rscale * d
+// ---- classic PCG (one recurrence, r; the dots p.Ap and r.z come fused out
+// of the SpMVs that produce Ap and z) ----------------------------------------
+
+// Set the stop / replacement flags after the residual update.
+__device__ __forceinline__ void cg_flags(PcgState *st, double rr)
+{
+  if (!isfinite(rr))
+    st->done = kBreakdown;
+  else if (rr <= st->thresh2)
+    st->done = kConverged;
+  else if (rr < st->ru2 * st->rr_ref)
+    st->done = kReplace;
+  else if (st->it >= st->max_it)
+    st->done = kCap;
+}
+
+// alpha = rz / pq; d += alpha p; r -= alpha q; rr = ||r||^2
 template <class T>
 __global__ void __launch_bounds__(kThreads)
-    apply_correction_kernel(double *__restrict__ x, const T *__restrict__ d, long long n,
-                            const PcgState *st)
+    cg_update_kernel(const T *__restrict__ p, const T *__restrict__ q, T *__restrict__ r,
+                     T *__restrict__ d, long long n, PcgState *st, Scratch sc, int noprec)
 {
-  const double sc = st->rscale;
-  GRID_STRIDE(i, n) x[i] = fma(sc, (double)d[i], x[i]);
+  if (st->done)
+    return;
+  const double alpha = st->rz / st->pq;
+  if (!(alpha > 0.0) || !isfinite(alpha)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+      st->done = kBreakdown;
+    return;
+  }
+  const T a = (T)alpha;
+  Acc<1> acc{{0.0}};
+  GRID_STRIDE(i, n)
+  {
+    T ri = fma(-a, q[i], r[i]);
+    r[i] = ri;
+    d[i] = fma(a, p[i], d[i]);
+    acc.v[0] = fma((double)ri, (double)ri, acc.v[0]);
+  }
+  Acc<1> tot;
+  if (grid_total<1>(acc, sc, tot) && threadIdx.x == 0) {
+    st->alpha = alpha;
+    st->rr = tot.v[0];
+    if (noprec)
+      st->rz_new = tot.v[0];
+    st->it += 1;
+    cg_flags(st, tot.v[0]);
+  }
+}
+
+// beta = rz_new / rz (0 on a fresh start); p = z + beta p; rz = rz_new
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+    cg_direction_kernel(const T *__restrict__ z, T *__restrict__ p, long long n, PcgState *st,
+                        Scratch sc)
+{
+  if (st->done)
+    return;
+  const bool fresh = st->fresh;
+  const double rzn = st->rz_new;
+  const double beta = fresh ? 0.0 : rzn / st->rz;
+  if (!(rzn > 0.0) || !isfinite(beta)) {
+    // M is not positive definite on this residual (or r vanished exactly)
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+      st->done = rzn == 0.0 ? kConverged : kBreakdown;
+    return;
+  }
+  const T b = (T)beta;
+  if (fresh) {
+    GRID_STRIDE(i, n) p[i] = z[i];
+  } else {
+    GRID_STRIDE(i, n) p[i] = fma(b, p[i], z[i]);
+  }
+  Acc<1> none{{0.0}}, tot;
+  if (grid_total<1>(none, sc, tot) && threadIdx.x == 0) {
+    st->beta = beta;
+    st->rz = rzn;
+    st->fresh = 0;
+  }
+}
+
+// r = (T) r64 (0 on padding), d = 0, rr = ||r||^2; arms the phase.
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+    cg_load_kernel(const double *__restrict__ r64, T *r, T *d, long long n, long long n_pad,
+                   PcgState *st, Scratch sc, double thresh2, double ru2, int max_it,
+                   int restart, int noprec)
+{
+  Acc<1> acc{{0.0}};
+  GRID_STRIDE(i, n_pad)
+  {
+    T ri = i < n ? (T)r64[i] : T(0);
+    r[i] = ri;
+    d[i] = T(0);
+    acc.v[0] = fma((double)ri, (double)ri, acc.v[0]);
+  }
+  Acc<1> tot;
+  if (grid_total<1>(acc, sc, tot) && threadIdx.x == 0) {
+    st->rr = tot.v[0];
+    st->rr_ref = tot.v[0];
+    st->thresh2 = thresh2;
+    st->ru2 = ru2;
+    st->max_it = max_it;
+    if (noprec)
+      st->rz_new = tot.v[0];
+    if (restart) {
+      st->it = 0;
+      st->fresh = 1;
+    }
+    st->done = tot.v[0] <= thresh2 ? kConverged : kRunning;
+  }
 }
 
 int grid_for(long long n)
@@ -288,14 +423,14 @@ struct DevMem {
   template <class T> int get(T **out, size_t count)
   {
     void *p = nullptr;
-    cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T) + 256);
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T) + 256;
+    cudaError_t e = cudaMalloc(&p, bytes);
     if (e != cudaSuccess) {
       cudaGetLastError();
-      return fail(ISPM_ERR_NOMEM, "solver cudaMalloc(%zu): %s", count * sizeof(T),
-                  cudaGetErrorString(e));
+      return fail(ISPM_ERR_NOMEM, "solver cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
     }
     blocks.push_back(p);
-    e = cudaMemset(p, 0, std::max<size_t>(count, 1) * sizeof(T) + 256);
+    e = cudaMemset(p, 0, bytes);
     if (e != cudaSuccess)
       return fail(ISPM_ERR_CUDA, "cudaMemset: %s", cudaGetErrorString(e));
     *out = (T *)p;
@@ -337,7 +472,6 @@ void reverse_cols(int n, const int *rp, const int *ci, const double *v, std::vec
 }
 
 struct Operator {
-  HostSlell host;
   DeviceSlell dev;
   ispm_launch_params lp{};
   int upload(int vec_dtype, int elm_dtype, int n, const int *rp, const int *ci,
@@ -354,22 +488,21 @@ struct Operator {
     }
     if (int st = guess_format(elm_dtype, n, n, rp, ci, vals, 1, 4, f))
       return st;
+    HostSlell host;
     if (int st = convert_csr(elm_dtype, n, n, rp, ci, vals, (int)f.S, (int)f.H, f.V != 0,
                              f.D != 0, 4, host))
       return st;
     if (int st = dev.upload(host))
       return st;
     lp = default_launch(vec_dtype, dev.view());
-    // drop the host copy: the device matrix is all the solver needs
-    HostSlell keep_meta;
-    keep_meta.n_rows = host.n_rows;
-    host = std::move(keep_meta);
     return ISPM_OK;
   }
-  int apply(int vdt, const void *x, void *y, cudaStream_t s, const int *skip) const
+  int apply(int vdt, const void *x, void *y, cudaStream_t s, const int *skip,
+            const SpmvDot *ep = nullptr) const
   {
-    return launch_spmv(vdt, lp, dev.view(), x, y, s, skip);
+    return launch_spmv(vdt, lp, dev.view(), x, y, s, skip, ep);
   }
+  unsigned grid() const { return spmv_grid(lp, dev.view()); }
 };
 
 }  // namespace
@@ -384,11 +517,22 @@ struct Solver {
   PcgState *st = nullptr;
   PcgState *st_host = nullptr;  // pinned mirror
   Scratch sc{};
+  unsigned part_capacity = 0;  // partial slots in sc.part
+  bool classic = false;        // classic PCG instead of the pipelined recurrence
   double *x64 = nullptr, *r64 = nullptr, *t64 = nullptr, *b64 = nullptr;
-  void *vec[11] = {};  // r u w m n p s q z d t (inner type)
+  double *b_stage = nullptr, *x_stage = nullptr;  // device copies for host-vector solves
+  void *vec[11] = {};
+  enum { R, U, W, M, NV, P, S, Q, Z, D, TT };
   cudaGraphExec_t graph = nullptr;
-  cudaStream_t graph_stream = nullptr;
+  // The solve runs on the solver's own stream (the legacy default stream
+  // cannot be captured into a graph), ordered after / before the caller's
+  // stream with two events.
+  cudaStream_t own = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   std::vector<double> history;
+  int replacements = 0, restarts = 0;
+  // ISPM_SOLVER_VERBOSE=1: one stderr line per solver phase (diagnostics)
+  bool verbose = getenv("ISPM_SOLVER_VERBOSE") && atoi(getenv("ISPM_SOLVER_VERBOSE")) > 0;
 
   ~Solver()
   {
@@ -396,55 +540,130 @@ struct Solver {
       cudaGraphExecDestroy(graph);
     if (st_host)
       cudaFreeHost(st_host);
+    if (ev_in)
+      cudaEventDestroy(ev_in);
+    if (ev_out)
+      cudaEventDestroy(ev_out);
+    if (own)
+      cudaStreamDestroy(own);
   }
 
-  void *V(int k) const { return vec[k]; }
-  enum { R, U, W, M, NV, P, S, Q, Z, D, TT };
+  size_t esize() const { return inner == ISPM_F32 ? 4 : 8; }
 
-  int prec_apply(const void *in, void *out, cudaStream_t s, const int *skip)
+  int init_stream()
   {
-    if (!have_prec)
-      return ISPM_ERR_INVALID;
+    ISPM_CUDA_TRY(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
+    ISPM_CUDA_TRY(cudaEventCreateWithFlags(&ev_in, cudaEventDisableTiming));
+    ISPM_CUDA_TRY(cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming));
+    return ISPM_OK;
+  }
+
+  int launched(const char *what)
+  {
+    cudaError_t e = cudaPeekAtLastError();
+    return e == cudaSuccess ? ISPM_OK : fail(ISPM_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  }
+
+  // out = M in (two SpMVs), or a copy without a preconditioner.
+  int prec(const void *in, void *out, cudaStream_t s, const int *skip)
+  {
+    if (!have_prec) {
+      ISPM_CUDA_TRY(cudaMemcpyAsync(out, in, (size_t)n_pad * esize(), cudaMemcpyDeviceToDevice, s));
+      return ISPM_OK;
+    }
     if (int e = G.apply(inner, in, vec[TT], s, skip))
       return e;
     return Ht.apply(inner, vec[TT], out, s, skip);
   }
 
-  template <class T> int launch_step(cudaStream_t s)
+  template <class T> int step(cudaStream_t s)
   {
-    const int grid = grid_for(n_pad);
-    pcg_step_kernel<T><<<grid, kThreads, 0, s>>>(
+    pcg_step_kernel<T><<<grid_for(n_pad), kThreads, 0, s>>>(
         (const T *)vec[NV], (const T *)vec[M], (T *)vec[P], (T *)vec[S], (T *)vec[Q],
         (T *)vec[Z], (T *)vec[D], (T *)vec[R], (T *)vec[U], (T *)vec[W], n_pad, st, sc);
-    cudaError_t e = cudaPeekAtLastError();
-    return e == cudaSuccess ? ISPM_OK : fail(ISPM_ERR_CUDA, "pcg step: %s", cudaGetErrorString(e));
+    return launched("pcg step");
   }
 
-  // One inner iteration: m = M w, n = A m, fused update.
+  // One iteration.  Pipelined: m = M w, n = A m, fused update.  Classic:
+  // q = A p (+ p.q), d/r update (+ r.r), z = M r (+ r.z), new direction.
   int iteration(cudaStream_t s)
   {
     const int *skip = &st->done;
-    if (have_prec) {
-      if (int e = prec_apply(vec[W], vec[M], s, skip))
-        return e;
-    } else {
-      ISPM_CUDA_TRY(cudaMemcpyAsync(vec[M], vec[W], (size_t)n_pad * esize(), cudaMemcpyDeviceToDevice, s));
-    }
+    if (classic)
+      return inner == ISPM_F32 ? cg_iteration<float>(s) : cg_iteration<double>(s);
+    if (int e = prec(vec[W], vec[M], s, skip))
+      return e;
     if (int e = Ain.apply(inner, vec[M], vec[NV], s, skip))
       return e;
-    return inner == ISPM_F32 ? launch_step<float>(s) : launch_step<double>(s);
+    return inner == ISPM_F32 ? step<float>(s) : step<double>(s);
   }
 
-  size_t esize() const { return inner == ISPM_F32 ? 4 : 8; }
+  SpmvDot dot_into(const void *v, double *out) const
+  {
+    SpmvDot ep;
+    ep.v = v;
+    ep.out = out;
+    ep.part = sc.part;
+    ep.ticket = sc.ticket;
+    ep.part_capacity = part_capacity;
+    return ep;
+  }
+
+  // z = M r with r.z fused into the last SpMV; without a preconditioner
+  // z = r and r.z was produced with r.r.
+  template <class T> int cg_precondition(cudaStream_t s, const int *skip)
+  {
+    if (!have_prec)
+      return ISPM_OK;
+    if (int e = G.apply(inner, vec[R], vec[TT], s, skip))
+      return e;
+    SpmvDot ep = dot_into(vec[R], &st->rz_new);
+    return Ht.apply(inner, vec[TT], vec[Z], s, skip, &ep);
+  }
+
+  template <class T> int cg_direction(cudaStream_t s)
+  {
+    const T *z = (const T *)(have_prec ? vec[Z] : vec[R]);
+    cg_direction_kernel<T><<<grid_for(n_pad), kThreads, 0, s>>>(z, (T *)vec[P], n_pad, st, sc);
+    return launched("cg direction");
+  }
+
+  template <class T> int cg_iteration(cudaStream_t s)
+  {
+    const int *skip = &st->done;
+    SpmvDot ep = dot_into(vec[P], &st->pq);
+    if (int e = Ain.apply(inner, vec[P], vec[Q], s, skip, &ep))
+      return e;
+    cg_update_kernel<T><<<grid_for(n_pad), kThreads, 0, s>>>(
+        (const T *)vec[P], (const T *)vec[Q], (T *)vec[R], (T *)vec[D], n_pad, st, sc,
+        have_prec ? 0 : 1);
+    if (int e = launched("cg update"))
+      return e;
+    if (int e = cg_precondition<T>(s, skip))
+      return e;
+    return cg_direction<T>(s);
+  }
+
+  // Classic-CG phase start: r from r64, then z = M r and the new direction
+  // (a fresh one on a restart, p = z + beta p after a reliable update).
+  template <class T>
+  int cg_resync(cudaStream_t s, bool restart, double thresh2, double ru2, int max_it)
+  {
+    cg_load_kernel<T><<<grid_for(n_pad), kThreads, 0, s>>>(
+        r64, (T *)vec[R], (T *)vec[D], n, n_pad, st, sc, thresh2, ru2, max_it, restart,
+        have_prec ? 0 : 1);
+    if (int e = launched("cg load"))
+      return e;
+    const int *skip = &st->done;
+    if (int e = cg_precondition<T>(s, skip))
+      return e;
+    return cg_direction<T>(s);
+  }
 
   int build_graph(cudaStream_t s)
   {
-    if (graph && graph_stream == s)
+    if (graph)
       return ISPM_OK;
-    if (graph) {
-      cudaGraphExecDestroy(graph);
-      graph = nullptr;
-    }
     cudaGraph_t g;
     ISPM_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     int err = ISPM_OK;
@@ -459,112 +678,150 @@ struct Solver {
     cudaGraphDestroy(g);
     if (e != cudaSuccess)
       return fail(ISPM_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
-    graph_stream = s;
     return ISPM_OK;
   }
 
-  template <class T> int start_inner(cudaStream_t s, double rel_tol, int max_it)
-  {
-    const int grid = grid_for(n_pad);
-    scale_rhs_kernel<T><<<grid, kThreads, 0, s>>>(r64, (T *)vec[R], (T *)vec[D], (T *)vec[P],
-                                                  (T *)vec[S], (T *)vec[Q], (T *)vec[Z], n,
-                                                  n_pad, st);
-    // u = M r, w = A u
-    if (have_prec) {
-      if (int e = prec_apply(vec[R], vec[U], s, nullptr))
-        return e;
-    } else {
-      ISPM_CUDA_TRY(cudaMemcpyAsync(vec[U], vec[R], (size_t)n_pad * sizeof(T), cudaMemcpyDeviceToDevice, s));
-    }
-    if (int e = Ain.apply(inner, vec[U], vec[W], s, nullptr))
-      return e;
-    init_dots_kernel<T><<<grid, kThreads, 0, s>>>((const T *)vec[R], (const T *)vec[U],
-                                                  (const T *)vec[W], n_pad, st, sc, rel_tol,
-                                                  max_it);
-    cudaError_t e = cudaPeekAtLastError();
-    return e == cudaSuccess ? ISPM_OK : fail(ISPM_ERR_CUDA, "inner start: %s", cudaGetErrorString(e));
-  }
-
-  int outer_residual(cudaStream_t s)
+  // r64 = b - A x64 and its norm (host copy of the state afterwards).
+  int true_residual(cudaStream_t s)
   {
     if (int e = A64.apply(ISPM_F64, x64, t64, s, nullptr))
       return e;
-    outer_residual_kernel<<<grid_for(n), kThreads, 0, s>>>(b64, t64, r64, n, st, sc);
-    ISPM_CUDA_TRY(cudaPeekAtLastError());
+    true_residual_kernel<<<grid_for(n), kThreads, 0, s>>>(b64, t64, r64, n, st, sc);
+    if (int e = launched("true residual"))
+      return e;
     ISPM_CUDA_TRY(cudaMemcpyAsync(st_host, st, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
     ISPM_CUDA_TRY(cudaStreamSynchronize(s));
     return ISPM_OK;
+  }
+
+  // Load r from r64 and re-derive the pipelined auxiliaries.  restart: also
+  // reset the search directions (first start, or after a breakdown).
+  template <class T>
+  int resync(cudaStream_t s, bool restart, double thresh2, double ru2, int max_it)
+  {
+    load_residual_kernel<T><<<grid_for(n_pad), kThreads, 0, s>>>(
+        r64, (T *)vec[R], (T *)vec[D], (T *)vec[P], (T *)vec[S], (T *)vec[Q], (T *)vec[Z], n,
+        n_pad, restart);
+    if (int e = launched("load residual"))
+      return e;
+    if (int e = prec(vec[R], vec[U], s, nullptr))  // u = M r
+      return e;
+    if (int e = Ain.apply(inner, vec[U], vec[W], s, nullptr))  // w = A u
+      return e;
+    if (!restart) {
+      if (int e = Ain.apply(inner, vec[P], vec[S], s, nullptr))  // s = A p
+        return e;
+      if (int e = prec(vec[S], vec[Q], s, nullptr))  // q = M s
+        return e;
+      if (int e = Ain.apply(inner, vec[Q], vec[Z], s, nullptr))  // z = A q
+        return e;
+    }
+    sync_dots_kernel<T><<<grid_for(n_pad), kThreads, 0, s>>>(
+        (const T *)vec[R], (const T *)vec[U], (const T *)vec[W], n_pad, st, sc, thresh2, ru2,
+        max_it, restart);
+    return launched("sync dots");
+  }
+
+  int fold(cudaStream_t s)
+  {
+    if (inner == ISPM_F32)
+      fold_correction_kernel<float><<<grid_for(n), kThreads, 0, s>>>(x64, (float *)vec[D], n);
+    else
+      fold_correction_kernel<double><<<grid_for(n), kThreads, 0, s>>>(x64, (double *)vec[D], n);
+    return launched("fold correction");
   }
 
   int solve(const double *b, double *x, ispm_solve_stats *stats, cudaStream_t s)
   {
     auto t0 = std::chrono::steady_clock::now();
     history.clear();
+    replacements = restarts = 0;
     b64 = const_cast<double *>(b);
     x64 = x;
-    ispm_solve_stats out{};
-    // ||b|| from the first outer residual with the caller's initial guess
-    // replaced by zero
-    ISPM_CUDA_TRY(cudaMemsetAsync(x64, 0, (size_t)n * sizeof(double), s));
-    if (int e = outer_residual(s))
+    ISPM_CUDA_TRY(cudaMemsetAsync(x64, 0, (size_t)n_pad * sizeof(double), s));
+    if (int e = true_residual(s))  // r64 = b
       return e;
     const double bnorm = std::sqrt(st_host->res2);
-    double rel = 1.0;
-    int total_it = 0, cycles = 0, status = ISPM_OK;
-    if (bnorm == 0.0) {
-      rel = 0.0;
-    }
-    const double eta_min = inner == ISPM_F32 ? opts.inner_tol_f32 : 0.0;
+    double rel = bnorm > 0 ? 1.0 : 0.0;
+    int total_it = 0, status = ISPM_OK;
+    const double target = opts.tol * bnorm;
+    // the recursive residual must get a little below the target so that the
+    // true residual (which it tracks to within the drift) meets it
+    const double thresh2 = 0.25 * target * target;
+    const double ru = inner == ISPM_F32 ? opts.replace_ratio_f32 : opts.replace_ratio_f64;
+    const double ru2 = ru * ru;
+    bool restart = true;
+    int since_restart = 0;
     while (rel > opts.tol) {
-      if (cycles >= opts.max_refinements || total_it >= opts.max_iters) {
+      if (replacements + restarts >= opts.max_refinements || total_it >= opts.max_iters) {
         status = ISPM_ERR_NOT_CONVERGED;
         break;
       }
-      // inner target: the outer goal (with margin), never tighter than FP32 allows
-      const double need = 0.5 * opts.tol / rel;
-      const double eta = std::max(need, eta_min);
-      const int budget = opts.max_iters - total_it;
-      int e = inner == ISPM_F32 ? start_inner<float>(s, eta, budget)
-                                : start_inner<double>(s, eta, budget);
+      const int budget = opts.max_iters - total_it + (restart ? 0 : since_restart);
+      int e;
+      if (classic)
+        e = inner == ISPM_F32 ? cg_resync<float>(s, restart, thresh2, ru2, budget)
+                              : cg_resync<double>(s, restart, thresh2, ru2, budget);
+      else
+        e = inner == ISPM_F32 ? resync<float>(s, restart, thresh2, ru2, budget)
+                              : resync<double>(s, restart, thresh2, ru2, budget);
       if (e)
         return e;
-      if (opts.use_graph)
-        if (int e2 = build_graph(s))
-          return e2;
+      if (restart)
+        since_restart = 0;
+      int done = kRunning;
       for (;;) {
+        ISPM_CUDA_TRY(cudaMemcpyAsync(st_host, st, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
+        ISPM_CUDA_TRY(cudaStreamSynchronize(s));
+        if (st_host->done) {
+          done = st_host->done;
+          break;
+        }
         if (opts.use_graph) {
+          if (int e2 = build_graph(s))
+            return e2;
           ISPM_CUDA_TRY(cudaGraphLaunch(graph, s));
         } else {
           for (int k = 0; k < opts.check_every; k++)
             if (int e3 = iteration(s))
               return e3;
         }
-        ISPM_CUDA_TRY(cudaMemcpyAsync(st_host, st, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
-        ISPM_CUDA_TRY(cudaStreamSynchronize(s));
-        if (st_host->done)
-          break;
       }
-      total_it += st_host->it;
-      cycles++;
-      if (inner == ISPM_F32)
-        apply_correction_kernel<float><<<grid_for(n), kThreads, 0, s>>>(x64, (const float *)vec[D], n, st);
-      else
-        apply_correction_kernel<double><<<grid_for(n), kThreads, 0, s>>>(x64, (const double *)vec[D], n, st);
-      ISPM_CUDA_TRY(cudaPeekAtLastError());
-      const int inner_done = st_host->done;
-      if (int e4 = outer_residual(s))
+      total_it += st_host->it - since_restart;
+      since_restart = st_host->it;
+      if (int e4 = fold(s))
         return e4;
-      double new_rel = std::sqrt(st_host->res2) / bnorm;
+      if (int e5 = true_residual(s))
+        return e5;
+      const double new_rel = std::sqrt(st_host->res2) / bnorm;
       history.push_back(new_rel);
-      if (inner_done == 2 && !(new_rel < rel)) {
+      if (verbose)
+        fprintf(stderr,
+                "[ispm solver] %s phase end: done=%d it=%d total=%d recursive=%.3e "
+                "true=%.3e\n",
+                inner == ISPM_F32 ? "f32" : "f64", done, st_host->it, total_it,
+                std::sqrt(std::max(0.0, st_host->rr)) / bnorm, new_rel);
+      if (done == kBreakdown) {
+        restarts++;
+        restart = true;
+        if (!(new_rel < rel) && restarts > 2) {
+          rel = new_rel;
+          status = ISPM_ERR_BREAKDOWN;
+          break;
+        }
+      } else if (done == kCap) {
         rel = new_rel;
-        status = ISPM_ERR_BREAKDOWN;
+        status = ISPM_ERR_NOT_CONVERGED;
         break;
+      } else {
+        replacements++;
+        restart = false;
       }
       rel = new_rel;
     }
+    ispm_solve_stats out{};
     out.iterations = total_it;
-    out.refinements = cycles;
+    out.refinements = replacements + restarts;
     out.true_relres = rel;
     out.converged = rel <= opts.tol;
     out.status = status;
@@ -574,6 +831,21 @@ struct Solver {
     if (status != ISPM_OK)
       return fail(status, "solve stopped at relative residual %.3e after %d iterations", rel,
                   total_it);
+    return ISPM_OK;
+  }
+
+  int solve_on(const double *b, double *x, ispm_solve_stats *stats, cudaStream_t user)
+  {
+    ISPM_CUDA_TRY(cudaEventRecord(ev_in, user));
+    ISPM_CUDA_TRY(cudaStreamWaitEvent(own, ev_in, 0));
+    int e = solve(b, x, stats, own);
+    cudaError_t ce = cudaEventRecord(ev_out, own);
+    if (ce == cudaSuccess)
+      ce = cudaStreamWaitEvent(user, ev_out, 0);
+    if (e)
+      return e;
+    if (ce != cudaSuccess)
+      return fail(ISPM_ERR_CUDA, "stream join: %s", cudaGetErrorString(ce));
     return ISPM_OK;
   }
 };
@@ -595,10 +867,12 @@ void ispm_solver_default_opts(ispm_solver_opts *o)
   o->inner_dtype = ISPM_F32;
   o->tol = 1e-10;
   o->max_iters = 100000;
-  o->max_refinements = 50;
+  o->max_refinements = 500;
   o->check_every = 16;
-  o->inner_tol_f32 = 1e-5;
   o->use_graph = 1;
+  o->replace_ratio_f32 = 1e-1;
+  o->replace_ratio_f64 = 1e-4;
+  o->variant = ISPM_PCG_AUTO;
 }
 
 int ispm_solver_create(int n, const int *row_ptr, const int *cols, const double *vals,
@@ -622,7 +896,16 @@ int ispm_solver_create(int n, const int *row_ptr, const int *cols, const double 
     return fail(ISPM_ERR_INVALID, "inner_dtype %d", S.opts.inner_dtype);
   if (S.opts.check_every < 1 || S.opts.check_every > 4096)
     return fail(ISPM_ERR_INVALID, "check_every %d", S.opts.check_every);
+  if (!(S.opts.replace_ratio_f32 > 0 && S.opts.replace_ratio_f32 < 1) ||
+      !(S.opts.replace_ratio_f64 > 0 && S.opts.replace_ratio_f64 < 1))
+    return fail(ISPM_ERR_INVALID, "replacement ratios must lie in (0, 1)");
   S.inner = S.opts.inner_dtype;
+  if (S.opts.variant == ISPM_PCG_AUTO)
+    S.classic = S.inner == ISPM_F32;
+  else if (S.opts.variant == ISPM_PCG_CLASSIC || S.opts.variant == ISPM_PCG_PIPELINED)
+    S.classic = S.opts.variant == ISPM_PCG_CLASSIC;
+  else
+    return fail(ISPM_ERR_INVALID, "variant %d", S.opts.variant);
   S.n = n;
   S.have_prec = g1_rp && g2_rp;
   try {
@@ -644,19 +927,25 @@ int ispm_solver_create(int n, const int *row_ptr, const int *cols, const double 
     return fail(ISPM_ERR_NOMEM, "host allocation while building the solver");
   }
   S.n_pad = S.A64.dev.meta.n_rows;
+  if (int e = S.init_stream())
+    return e;
   const size_t npad = (size_t)S.n_pad + 64;
   if (int e = S.mem.get(&S.st, 1))
     return e;
   if (cudaMallocHost(&S.st_host, sizeof(PcgState)) != cudaSuccess)
     return fail(ISPM_ERR_NOMEM, "pinned host allocation");
-  if (int e = S.mem.get(&S.sc.part, 4 * kMaxBlocks))
+  // partial slots: the fixed-grid kernels use 4 * kMaxBlocks, a fused SpMV
+  // dot one per CTA of that SpMV
+  S.part_capacity = std::max<unsigned>(
+      {4u * kMaxBlocks, S.Ain.grid(), S.have_prec ? S.Ht.grid() : 0u});
+  if (int e = S.mem.get(&S.sc.part, S.part_capacity))
     return e;
   if (int e = S.mem.get(&S.sc.ticket, 4))
     return e;
-  if (int e = S.mem.get(&S.r64, npad))
-    return e;
-  if (int e = S.mem.get(&S.t64, npad))
-    return e;
+  double **d64[] = {&S.r64, &S.t64, &S.b_stage, &S.x_stage};
+  for (double **pp : d64)
+    if (int e = S.mem.get(pp, npad))
+      return e;
   for (int k = 0; k < 11; k++) {
     int e = S.inner == ISPM_F32 ? S.mem.get((float **)&S.vec[k], npad)
                                 : S.mem.get((double **)&S.vec[k], npad);
@@ -675,7 +964,7 @@ int ispm_solver_solve(ispm_solver *s, const double *b, double *x, ispm_solve_sta
   clear_error();
   if (!s || !b || !x)
     return fail(ISPM_ERR_INVALID, "NULL argument");
-  return s->s.solve(b, x, stats, (cudaStream_t)stream);
+  return s->s.solve_on(b, x, stats, (cudaStream_t)stream);
 }
 
 int ispm_solver_solve_host(ispm_solver *s, const double *b_host, double *x_host,
@@ -686,20 +975,11 @@ int ispm_solver_solve_host(ispm_solver *s, const double *b_host, double *x_host,
     return fail(ISPM_ERR_INVALID, "NULL argument");
   Solver &S = s->s;
   cudaStream_t st = (cudaStream_t)stream;
-  double *b = nullptr, *x = nullptr;
-  if (int e = S.mem.get(&b, S.n_pad + 64))
-    return e;
-  if (int e = S.mem.get(&x, S.n_pad + 64))
-    return e;
-  ISPM_CUDA_TRY(cudaMemcpyAsync(b, b_host, (size_t)S.n * 8, cudaMemcpyHostToDevice, st));
-  int e = S.solve(b, x, stats, st);
-  cudaError_t ce = cudaMemcpyAsync(x_host, x, (size_t)S.n * 8, cudaMemcpyDeviceToHost, st);
-  cudaStreamSynchronize(st);
-  // release the two staging vectors
-  for (int k = 0; k < 2; k++) {
-    cudaFree(S.mem.blocks.back());
-    S.mem.blocks.pop_back();
-  }
+  ISPM_CUDA_TRY(cudaMemcpyAsync(S.b_stage, b_host, (size_t)S.n * 8, cudaMemcpyHostToDevice, st));
+  int e = S.solve_on(S.b_stage, S.x_stage, stats, st);
+  cudaError_t ce = cudaMemcpyAsync(x_host, S.x_stage, (size_t)S.n * 8, cudaMemcpyDeviceToHost, st);
+  if (ce == cudaSuccess)
+    ce = cudaStreamSynchronize(st);
   if (e)
     return e;
   if (ce != cudaSuccess)

@@ -41,7 +41,52 @@ template <class T, class E> struct SpmvArgs {
   int x_vec_ok;       // x aligned for W-wide vector loads
   int x_al16;         // x 16-byte aligned (diagonal-window vector loads)
   const int *skip;    // optional device flag: nonzero -> the launch does nothing
+  SpmvDot ep;         // optional fused epilogue: *ep.out = sum_i y_i v_i (FP64)
 };
+
+// Block-wide FP64 sum; valid in thread 0.  blockDim.x <= 1024.
+__device__ __forceinline__ double block_sum_f64(double v)
+{
+  __shared__ double sh[32];
+  for (int off = 16; off > 0; off >>= 1)
+    v += __shfl_down_sync(0xffffffffu, v, off);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0)
+    sh[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    v = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+    for (int off = 16; off > 0; off >>= 1)
+      v += __shfl_down_sync(0xffffffffu, v, off);
+  }
+  return v;
+}
+
+// Finish a fused dot product: every block publishes its partial, the last
+// block to arrive adds them in block order (deterministic) and stores it.
+__device__ __forceinline__ void finish_dot(double v, const SpmvDot &ep)
+{
+  __shared__ bool last;
+  v = block_sum_f64(v);
+  if (threadIdx.x == 0) {
+    ep.part[blockIdx.x] = v;
+    __threadfence();
+    last = atomicAdd(ep.ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last)
+    return;
+  __threadfence();
+  double s = 0.0;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+    s += __ldcg(ep.part + b);
+  s = block_sum_f64(s);
+  if (threadIdx.x == 0) {
+    *ep.out = s;
+    *ep.ticket = 0u;
+  }
+}
 
 // Gather x[c*W .. c*W+W-1] into xw, zero beyond n_cols.
 template <class T, int W>
@@ -252,6 +297,17 @@ __global__ void __launch_bounds__(1024) slell_spmv_kernel(SpmvArgs<T, E> a)
   }
   if (active && t < R)
     st_vec<H, T>(a.y + y0 + t * H, acc);
+  if (a.ep.out) {
+    // fused y.v for the solver (the dot the next recurrence step needs)
+    double dv = 0.0;
+    if (active && t < R) {
+      const T *v = static_cast<const T *>(a.ep.v) + y0 + t * H;
+#pragma unroll
+      for (int h = 0; h < H; h++)
+        dv = fma((double)acc[h], (double)v[h], dv);
+    }
+    finish_dot(dv, a.ep);
+  }
 }
 
 template <class T, class E, int H, int W, bool VAR, bool DIAG>
@@ -292,10 +348,18 @@ int launch_h(const SpmvArgs<T, E> &args, const ispm_slell_view &m, unsigned tps,
 
 template <class T, class E>
 int launch_te(const ispm_launch_params &p, const ispm_slell_view &m, const void *x, void *y,
-              cudaStream_t s, const int *skip)
+              cudaStream_t s, const int *skip, const SpmvDot *ep)
 {
   SpmvArgs<T, E> a;
   a.skip = skip;
+  a.ep = ep ? *ep : SpmvDot{};
+  if (ep && ep->out) {
+    const unsigned block = p.N >= 256 ? p.N : 256;
+    const unsigned grid = (m.n_slices + block / p.N - 1) / (block / p.N);
+    if (grid > ep->part_capacity)
+      return fail(ISPM_ERR_INVALID, "fused dot needs %u partial slots, has %u", grid,
+                  ep->part_capacity);
+  }
   a.sp = m.slice_ptr;
   a.cols = m.cols;
   a.elms = static_cast<const E *>(m.elms);
@@ -359,19 +423,34 @@ int check_launch(int x_dtype, const ispm_launch_params &p, const ispm_slell_view
   return ISPM_OK;
 }
 
+unsigned spmv_grid(const ispm_launch_params &p, const ispm_slell_view &m)
+{
+  const unsigned block = p.N >= 256 ? p.N : 256;
+  const unsigned spb = block / p.N;
+  return (m.n_slices + spb - 1) / spb;
+}
+
 int launch_spmv(int x_dtype, const ispm_launch_params &p, const ispm_slell_view &m,
-                const void *x, void *y, cudaStream_t s, const int *skip)
+                const void *x, void *y, cudaStream_t s, const int *skip, const SpmvDot *ep)
 {
   int st = check_launch(x_dtype, p, m);
-  if (st || m.n_slices == 0)
+  if (st)
     return st;
+  if (m.n_slices == 0) {
+    if (ep && ep->out) {
+      cudaError_t e = cudaMemsetAsync(ep->out, 0, sizeof(double), s);
+      if (e != cudaSuccess)
+        return fail(ISPM_ERR_CUDA, "memset: %s", cudaGetErrorString(e));
+    }
+    return ISPM_OK;
+  }
   if (!x || !y || !m.slice_ptr || (m.n_elms && (!m.elms)) || (m.n_cols_arr && !m.cols))
     return fail(ISPM_ERR_INVALID, "NULL pointer");
   if (x_dtype == ISPM_F32)
-    return launch_te<float, float>(p, m, x, y, s, skip);
+    return launch_te<float, float>(p, m, x, y, s, skip, ep);
   if (m.elm_dtype == ISPM_F32)
-    return launch_te<double, float>(p, m, x, y, s, skip);
-  return launch_te<double, double>(p, m, x, y, s, skip);
+    return launch_te<double, float>(p, m, x, y, s, skip, ep);
+  return launch_te<double, double>(p, m, x, y, s, skip, ep);
 }
 
 }  // namespace ispm

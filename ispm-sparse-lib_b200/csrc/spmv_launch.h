@@ -10,10 +10,25 @@ namespace ispm {
 
 // Validate launch parameters against a matrix (no CUDA calls).
 int check_launch(int x_dtype, const ispm_launch_params &p, const ispm_slell_view &m);
+// Optional fused epilogue of an SpMV: *out = sum_i y_i v_i in FP64 over the
+// rows the launch writes (v has the vector type T).  part holds one partial
+// per CTA (part_capacity slots), ticket is a zero-initialised arrival counter
+// the launch leaves at zero.
+struct SpmvDot {
+  const void *v = nullptr;
+  double *out = nullptr;
+  double *part = nullptr;
+  unsigned *ticket = nullptr;
+  unsigned part_capacity = 0;
+};
+
 // Validate and launch y = A x on `s`.  `skip` (device int, may be NULL): the
 // kernel returns at once when it holds a nonzero value.
 int launch_spmv(int x_dtype, const ispm_launch_params &p, const ispm_slell_view &m,
-                const void *x, void *y, cudaStream_t s, const int *skip = nullptr);
+                const void *x, void *y, cudaStream_t s, const int *skip = nullptr,
+                const SpmvDot *ep = nullptr);
+// CTAs a launch of matrix m with params p uses (partials a fused dot needs).
+unsigned spmv_grid(const ispm_launch_params &p, const ispm_slell_view &m);
 
 // Device-resident sliced-ELL matrix.
 struct DeviceSlell {

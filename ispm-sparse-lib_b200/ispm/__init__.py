@@ -568,7 +568,8 @@ class sblas:
 class solver_opts(C.Structure):
     _fields_ = [("inner_dtype", C.c_int), ("tol", C.c_double), ("max_iters", C.c_int),
                 ("max_refinements", C.c_int), ("check_every", C.c_int),
-                ("inner_tol_f32", C.c_double), ("use_graph", C.c_int)]
+                ("use_graph", C.c_int), ("replace_ratio_f32", C.c_double),
+                ("replace_ratio_f64", C.c_double), ("variant", C.c_int)]
 
 
 class solve_stats(C.Structure):
@@ -611,19 +612,25 @@ class PCGSolver:
 
     A: FP64 csr_matrix (SPD).  G1, G2: the fastainv_sym pair (Ainv1, Ainv2) or
     None.  inner: np.float64 (plain FP64) or np.float32 (mixed precision: FP32
-    matrices / vectors, FP64 reductions, FP64 outer residual)."""
+    matrices / vectors, FP64 reductions).  Reliable updates recompute the
+    true residual with the FP64 matrix whenever the recursive residual has
+    fallen by replace_ratio since the previous one."""
 
     def __init__(self, A: csr_matrix, G1: csr_matrix | None = None,
                  G2: csr_matrix | None = None, inner=np.float32, tol: float = 1e-10,
-                 max_iters: int = 100000, max_refinements: int = 50, check_every: int = 16,
-                 inner_tol_f32: float = 1e-5, use_graph: bool = True):
+                 max_iters: int = 100000, max_refinements: int = 500,
+                 check_every: int = 16, use_graph: bool = True,
+                 replace_ratio: float | None = None, variant: str = "auto"):
         _declare_solver()
         L = _lib()
         o = solver_opts()
         L.ispm_solver_default_opts(C.byref(o))
         o.inner_dtype = F64 if np.dtype(inner) == np.float64 else F32
         o.tol, o.max_iters, o.max_refinements = tol, max_iters, max_refinements
-        o.check_every, o.inner_tol_f32, o.use_graph = check_every, inner_tol_f32, int(use_graph)
+        o.check_every, o.use_graph = check_every, int(use_graph)
+        if replace_ratio is not None:
+            o.replace_ratio_f32 = o.replace_ratio_f64 = replace_ratio
+        o.variant = {"auto": 0, "pipelined": 1, "classic": 2}[variant]
         if A.elms.dtype != np.float64:
             raise TypeError("the solver takes the FP64 matrix")
         self._keep = [A, G1, G2]

@@ -41,6 +41,33 @@ def test_pcg_c1_true_residual(ispm, oracle, cuda, c1, inner, tol):
         assert abs(st["iterations"] - it_cpu) <= max(3, 0.05 * it_cpu), (st, it_cpu)
 
 
+@pytest.mark.parametrize("inner,variant", [(np.float64, "classic"), (np.float32, "pipelined")])
+def test_pcg_other_variants(ispm, oracle, cuda, c1, inner, variant):
+    """Classic PCG in FP64 and pipelined PCG in FP32 (with reliable updates)
+    on config 1 also reach 1e-10 in the true residual."""
+    A, b, G1, G2 = c1
+    s = ispm.PCGSolver(A, G1, G2, inner=inner, tol=1e-10, variant=variant)
+    x, st = s.solve_host(b)
+    assert st["converged"], st
+    assert true_relres(oracle, A, b, x) <= 1e-10 * 1.001
+
+
+def test_pcg_mixed_matches_fp64_iterations(ispm, oracle, cuda, gen):
+    """FP32 classic PCG with FP64 reliable updates needs about the FP64
+    iteration count on a 27-point GRF system (kappa ~ 1e6)."""
+    A = gen.stencil_grf(32, 27, 8.0, 1.5, 0)
+    x_true = np.random.default_rng(0).uniform(-1, 1, A.n_rows)
+    b = oracle.csr_spmv_f64(A.row_ptr, A.cols, A.elms, x_true)
+    G1, G2 = ispm.fastainv_sym(A, np.float64, None, 200_000_000, 0.01)
+    its = {}
+    for inner in (np.float64, np.float32):
+        x, st = ispm.PCGSolver(A, G1, G2, inner=inner, tol=1e-10).solve_host(b)
+        assert st["converged"], st
+        assert true_relres(oracle, A, b, x) <= 1e-10 * 1.001
+        its[inner] = st["iterations"]
+    assert its[np.float32] <= 1.1 * its[np.float64] + 5, its
+
+
 def test_pcg_device_vectors_graph_and_eager_agree(ispm, oracle, cuda, c1):
     A, b, G1, G2 = c1
     outs = []
