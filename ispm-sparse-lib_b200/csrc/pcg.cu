@@ -136,6 +136,16 @@ template <int NV> __device__ bool grid_total(Acc<NV> a, Scratch sc, Acc<NV> &tot
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (n); \
        i += (long long)gridDim.x * blockDim.x)
 
+template <class T> struct Vec16;
+template <> struct Vec16<float> {
+  using type = float4;
+  static constexpr int n = 4;
+};
+template <> struct Vec16<double> {
+  using type = double2;
+  static constexpr int n = 2;
+};
+
 // x += d (FP64 iterate, correction in T), d = 0; then r64 = b - A x needs the
 // SpMV, done separately.
 template <class T>
@@ -325,12 +335,23 @@ __global__ void __launch_bounds__(kThreads)
   }
   const T a = (T)alpha;
   Acc<1> acc{{0.0}};
-  GRID_STRIDE(i, n)
+  // 128-bit words: n is a multiple of 512 and the vectors are cudaMalloc'd
+  using V = typename Vec16<T>::type;
+  constexpr int K = Vec16<T>::n;
+  GRID_STRIDE(i, n / K)
   {
-    T ri = fma(-a, q[i], r[i]);
-    r[i] = ri;
-    d[i] = fma(a, p[i], d[i]);
-    acc.v[0] = fma((double)ri, (double)ri, acc.v[0]);
+    V pv = reinterpret_cast<const V *>(p)[i], qv = __ldcs(reinterpret_cast<const V *>(q) + i);
+    V rv = reinterpret_cast<const V *>(r)[i], dv = reinterpret_cast<const V *>(d)[i];
+    T *P = reinterpret_cast<T *>(&pv), *Q = reinterpret_cast<T *>(&qv);
+    T *Rr = reinterpret_cast<T *>(&rv), *D = reinterpret_cast<T *>(&dv);
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      Rr[k] = fma(-a, Q[k], Rr[k]);
+      D[k] = fma(a, P[k], D[k]);
+      acc.v[0] = fma((double)Rr[k], (double)Rr[k], acc.v[0]);
+    }
+    reinterpret_cast<V *>(r)[i] = rv;
+    reinterpret_cast<V *>(d)[i] = dv;
   }
   Acc<1> tot;
   if (grid_total<1>(acc, sc, tot) && threadIdx.x == 0) {
@@ -361,10 +382,21 @@ __global__ void __launch_bounds__(kThreads)
     return;
   }
   const T b = (T)beta;
+  using V = typename Vec16<T>::type;
+  constexpr int K = Vec16<T>::n;
   if (fresh) {
-    GRID_STRIDE(i, n) p[i] = z[i];
+    GRID_STRIDE(i, n / K)
+    reinterpret_cast<V *>(p)[i] = reinterpret_cast<const V *>(z)[i];
   } else {
-    GRID_STRIDE(i, n) p[i] = fma(b, p[i], z[i]);
+    GRID_STRIDE(i, n / K)
+    {
+      V zv = reinterpret_cast<const V *>(z)[i], pv = reinterpret_cast<const V *>(p)[i];
+      T *Z = reinterpret_cast<T *>(&zv), *P = reinterpret_cast<T *>(&pv);
+#pragma unroll
+      for (int k = 0; k < K; k++)
+        P[k] = fma(b, P[k], Z[k]);
+      reinterpret_cast<V *>(p)[i] = pv;
+    }
   }
   Acc<1> none{{0.0}}, tot;
   if (grid_total<1>(none, sc, tot) && threadIdx.x == 0) {
@@ -409,7 +441,8 @@ __global__ void __launch_bounds__(kThreads)
 int grid_for(long long n)
 {
   long long blocks = (n + kThreads - 1) / kThreads;
-  long long cap = std::min<long long>(kMaxBlocks, (long long)device_sm_count() * 4);
+  // about one full wave of 256-thread CTAs (8 per SM) for the streaming kernels
+  long long cap = std::min<long long>(kMaxBlocks, (long long)device_sm_count() * 8);
   return (int)std::max(1LL, std::min(blocks, cap));
 }
 
@@ -474,10 +507,15 @@ void reverse_cols(int n, const int *rp, const int *ci, const double *v, std::vec
 struct Operator {
   DeviceSlell dev;
   ispm_launch_params lp{};
+  ispm_slell_params fmt{};
+
+  // Store the operator in the sliced-ELL shape with the fewest bytes among
+  // the reference's guess and a few fixed shapes (the guess samples only the
+  // first 1% of rows, which misjudges the FSAI factors: their first rows are
+  // the shortest).  `force` skips the search (same pattern, other precision).
   int upload(int vec_dtype, int elm_dtype, int n, const int *rp, const int *ci,
-             const double *v)
+             const double *v, const ispm_slell_params *force = nullptr)
   {
-    ispm_slell_params f;
     std::vector<float> vf;
     const void *vals = v;
     if (elm_dtype == ISPM_F32) {
@@ -486,13 +524,38 @@ struct Operator {
         vf[k] = (float)v[k];
       vals = vf.data();
     }
-    if (int st = guess_format(elm_dtype, n, n, rp, ci, vals, 1, 4, f))
-      return st;
-    HostSlell host;
-    if (int st = convert_csr(elm_dtype, n, n, rp, ci, vals, (int)f.S, (int)f.H, f.V != 0,
-                             f.D != 0, 4, host))
-      return st;
-    if (int st = dev.upload(host))
+    std::vector<ispm_slell_params> cands;
+    if (force) {
+      cands.push_back(*force);
+    } else {
+      ispm_slell_params g;
+      if (int st = guess_format(elm_dtype, n, n, rp, ci, vals, 1, 4, g))
+        return st;
+      cands.push_back(g);
+      for (unsigned S : {32u, 64u, 128u})
+        for (unsigned D : {1u, 0u})
+          cands.push_back(ispm_slell_params{S, 1, 0, D});
+      cands.push_back(ispm_slell_params{64, 2, 0, 0});
+    }
+    const size_t esz = elm_dtype == ISPM_F32 ? 4 : 8;
+    HostSlell best;
+    size_t best_bytes = ~(size_t)0;
+    for (const ispm_slell_params &c : cands) {
+      HostSlell h;
+      if (convert_csr(elm_dtype, n, n, rp, ci, vals, (int)c.S, (int)c.H, c.V != 0, c.D != 0, 4,
+                      h))
+        continue;
+      const size_t bytes = 4 * h.slice_ptr.size() + 4 * h.cols.size() + esz * h.n_elms();
+      if (bytes < best_bytes) {
+        best_bytes = bytes;
+        best = std::move(h);
+        fmt = c;
+      }
+    }
+    clear_error();
+    if (best_bytes == ~(size_t)0)
+      return fail(ISPM_ERR_INVALID, "no sliced-ELL shape accepted the operator");
+    if (int st = dev.upload(best))
       return st;
     lp = default_launch(vec_dtype, dev.view());
     return ISPM_OK;
@@ -909,9 +972,9 @@ int ispm_solver_create(int n, const int *row_ptr, const int *cols, const double 
   S.n = n;
   S.have_prec = g1_rp && g2_rp;
   try {
-    if (int e = S.A64.upload(ISPM_F64, ISPM_F64, n, row_ptr, cols, vals))
-      return e;
     if (int e = S.Ain.upload(S.inner, S.inner, n, row_ptr, cols, vals))
+      return e;
+    if (int e = S.A64.upload(ISPM_F64, ISPM_F64, n, row_ptr, cols, vals, &S.Ain.fmt))
       return e;
     if (S.have_prec) {
       std::vector<int> rp, ci;
