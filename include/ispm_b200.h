@@ -211,6 +211,18 @@ int ispm_sblas_add_indexed(int dtype, void *dst, const void *src, const int *idx
                            void *stream);
 /* sblas::dot (sblas.cu:126-153): *s = sum x_i y_i. */
 int ispm_sblas_dot(int dtype, const void *x, const void *y, void *s, int n, void *stream);
+/* ispm_sblas_dot without any device allocation.  No counterpart in the
+ * reference: it is for callers that cannot let a library cudaMalloc (a fixed,
+ * pre-reserved device memory budget, or loops that must not risk the implicit
+ * synchronisation of cudaMalloc / cudaFree).  Same arguments and result as
+ * ispm_sblas_dot; its scratch is a static device array inside the library
+ * (1024 partial sums + a counter, about 8 KB per GPU, held until exit), so at
+ * most 1024 CTAs: devices with more than 256 SMs get ISPM_ERR_TOO_LARGE.  The
+ * first call on a device looks the array up (cudaGetSymbolAddress) -- make it
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU race. */
+int ispm_sblas_dot_noalloc(int dtype, const void *x, const void *y, void *s, int n,
+                           void *stream);
 /* sblas::ppcg_update_scalars (sblas.cu:156-174):
  * beta = gamma / gammaold; alpha = gamma / (delta - beta * gamma / alpha). */
 int ispm_sblas_ppcg_update_scalars(int dtype, void *alpha, void *beta, const void *gamma,
