@@ -185,6 +185,21 @@ int ispm_plan_update_device_matrix_coefs(ispm_plan *p);
  * with the plan's stored format parameters (host matrix only). */
 int ispm_plan_change_host_matrix(ispm_plan *p, int n_rows, int n_cols, const int *row_ptr,
                                  const int *cols, const void *elms);
+/* Device-side fast path of update_device_matrix_coefs / change_host_matrix
+ * for an unchanged sparsity pattern (plan/plan.h:39-56): new CSR values
+ * (device array, FP32 or FP64, in the CSR entry order of row_ptr / cols) are
+ * scattered straight into the device sliced-ELL matrix -- no host conversion,
+ * no host-to-device copy of the matrix.  The first call computes the entry ->
+ * slot map from the (host) pattern and keeps it on the device; later calls
+ * with the same nnz reuse it.  The plan's host matrix is not updated. */
+int ispm_plan_refresh_values(ispm_plan *p, int n_rows, const int *row_ptr, const int *cols,
+                             const void *vals_dev, int val_dtype, void *stream);
+/* The map itself (map[k] = element slot of CSR entry k, n_nz entries, host)
+ * and the scatter for callers managing device matrices directly. */
+int ispm_slell_value_map(const ispm_slell *m, int n_rows, const int *row_ptr, const int *cols,
+                         unsigned *map);
+int ispm_dslell_refresh_values(ispm_dslell *d, const unsigned *map_dev, const void *vals_dev,
+                               int val_dtype, int n_nz, void *stream);
 int ispm_plan_get_params(const ispm_plan *p, ispm_slell_params *mparams,
                          ispm_launch_params *params);
 /* The plan's matrices (NULL if absent); owned by the plan. */
@@ -260,6 +275,29 @@ int ispm_fastainv_sym(int out_dtype, int n, const int *row_ptr, const int *cols,
                       const double *elms, ispm_progress_f progress, void *v,
                       long long max_elts, double droptol, ispm_csr **ainv1, ispm_csr **ainv2,
                       ispm_fastainv_stats *stats);
+/* fastainv_sym with per-row controls (extends fastainv/fastainv.cpp:395-566;
+ * the plain entry point above is unchanged).  row_droptol[i] replaces droptol
+ * in the drop test of factor row i (fastainv.cpp:304), row_scale[j] > 0
+ * multiplies the pivot scale sqrt|D_jj| of factor row j in both outputs
+ * (fastainv.cpp:518-519), so M = Ainv2 Ainv1 = sum_j row_scale[j]^2 z_j z_j^T /
+ * D_jj.  Either array may be NULL (then droptol / 1).  Used by the learned
+ * FSAI, which predicts both per row. */
+int ispm_fastainv_sym_ex(int out_dtype, int n, const int *row_ptr, const int *cols,
+                         const double *elms, const double *row_droptol, const double *row_scale,
+                         long long max_elts, double droptol, ispm_csr **ainv1, ispm_csr **ainv2,
+                         ispm_fastainv_stats *stats);
+/* Factorized sparse approximate inverse built on the GPU: a parallel
+ * replacement for fastainv_sym's serial host build (fastainv.cpp:395-566),
+ * equivalent in PCG iterations rather than bit-identical.  G is lower
+ * triangular on A's lower pattern, each row solving A[P,P] y = e_i on the
+ * device; the pair is returned in fastainv_sym's convention, Ainv1 = G and
+ * Ainv2 = G^T, so that Ainv2 Ainv1 = G^T G ~ A^-1.  A: symmetric positive
+ * definite host CSR in FP64 with sorted columns, at most 32 entries per row
+ * at or left of the diagonal.  *fallbacks (may be NULL) counts rows whose
+ * local matrix was not positive definite (built as Jacobi rows). */
+int ispm_fsai_sym_gpu(int out_dtype, int n, const int *row_ptr, const int *cols,
+                      const double *elms, ispm_csr **ainv1, ispm_csr **ainv2,
+                      unsigned *fallbacks);
 int ispm_csr_get_info(const ispm_csr *m, int *n_rows, int *n_cols, int *n_nz, int *dtype);
 /* Host views of the CSR arrays; valid until ispm_csr_free. */
 int ispm_csr_get_arrays(const ispm_csr *m, const int **row_ptr, const int **cols,
@@ -283,7 +321,14 @@ typedef struct {
   double replace_ratio_f64; /* same for FP64 */
   int variant;          /* ISPM_PCG_AUTO (pipelined in FP64, classic in FP32),
                            ISPM_PCG_PIPELINED or ISPM_PCG_CLASSIC */
+  int prec;             /* ISPM_PREC_GIVEN: the (g1, g2) pair passed to
+                           ispm_solver_create (none if NULL); ISPM_PREC_FSAI_GPU:
+                           FSAI factor on A's lower pattern built on the GPU
+                           (g1, g2 ignored) */
 } ispm_solver_opts;
+
+#define ISPM_PREC_GIVEN 0
+#define ISPM_PREC_FSAI_GPU 1
 
 #define ISPM_PCG_AUTO 0
 #define ISPM_PCG_PIPELINED 1

@@ -145,15 +145,18 @@ struct SliceShape {
   long long cols_off = 0, elms_off = 0, diag_off = 0;
 };
 
-template <class E> struct Converter {
+// E is the matrix element type (it sizes the hblock cost model); V is what
+// lands in the element array -- E itself, or the CSR entry number when a
+// value-refresh map is built.
+template <class E, class V = E> struct Converter {
   CsrRows A;
-  const E *vals;
+  const V *vals;
   int hblock;
   bool diags;
   std::vector<SliceShape> shapes;
   std::vector<std::vector<int>> slice_diags;
   unsigned *cols_out = nullptr;
-  E *elms_out = nullptr;
+  V *elms_out = nullptr;
 
   void size_slice(SliceShape &s, std::vector<int> &diag, std::vector<int> &t1,
                   std::vector<int> &t2) const
@@ -315,10 +318,10 @@ template <class E> struct Converter {
   }
 };
 
-template <class E>
-int convert_impl(int n_rows, int n_cols, const int *row_ptr, const int *cols, const E *vals,
+template <class E, class V = E>
+int convert_impl(int n_rows, int n_cols, const int *row_ptr, const int *cols, const V *vals,
                  int S_req, int hblock, bool var_height, bool use_diags, int min_height,
-                 HostSlell &B, std::vector<E> &elms_vec)
+                 HostSlell &B, std::vector<V> &elms_vec)
 {
   const long long n_pad64 = ((long long)n_rows + kPadRows - 1) / kPadRows * kPadRows;
   if (n_pad64 > INT_MAX)
@@ -328,7 +331,7 @@ int convert_impl(int n_rows, int n_cols, const int *row_ptr, const int *cols, co
   if (hblock > 1)
     use_diags = false;
 
-  Converter<E> cv;
+  Converter<E, V> cv;
   cv.A = CsrRows{n_rows, n_pad, row_ptr, cols};
   cv.vals = vals;
   cv.hblock = hblock;
@@ -401,8 +404,9 @@ int convert_impl(int n_rows, int n_cols, const int *row_ptr, const int *cols, co
   B.diags = use_diags;
   B.max_slice_height = max_h;
   B.min_slice_height = min_h;
+  B.min_height_used = min_height;
   B.cols.assign(co, 0u);
-  elms_vec.assign(eo, E(0));
+  elms_vec.assign(eo, V(0));
   cv.cols_out = B.cols.data();
   cv.elms_out = elms_vec.data();
 
@@ -564,6 +568,41 @@ int convert_csr(int elm_dtype, int n_rows, int n_cols, const int *row_ptr, const
                               var_height, use_diags, min_height, out, out.elms_d);
 }
 
+int value_map(const HostSlell &m, int n_rows, const int *row_ptr, const int *cols,
+              std::vector<unsigned> &pos)
+{
+  // Convert again with the CSR entry numbers (1-based) as values and the
+  // matrix's own element type steering the hblock split: every entry lands
+  // where its value lands in m, so elms[p] = k + 1 gives pos[k] = p.
+  if (n_rows < 0 || !row_ptr || (row_ptr[n_rows] && !cols))
+    return fail(ISPM_ERR_INVALID, "bad CSR pattern");
+  const long long nnz = row_ptr[n_rows];
+  if ((long long)m.n_nz != nnz)
+    return fail(ISPM_ERR_INVALID, "pattern has %lld entries, the matrix %d", nnz, m.n_nz);
+  std::vector<long long> ids(nnz);
+  for (long long k = 0; k < nnz; k++)
+    ids[k] = k + 1;
+  HostSlell shape;
+  std::vector<long long> slots;
+  int st = m.elm_dtype == ISPM_F32
+               ? convert_impl<float, long long>(n_rows, m.n_cols, row_ptr, cols, ids.data(),
+                                                (int)m.slice_height, (int)m.hblock, m.var_height,
+                                                m.diags, (int)m.min_height_used, shape, slots)
+               : convert_impl<double, long long>(n_rows, m.n_cols, row_ptr, cols, ids.data(),
+                                                 (int)m.slice_height, (int)m.hblock,
+                                                 m.var_height, m.diags, (int)m.min_height_used,
+                                                 shape, slots);
+  if (st)
+    return st;
+  if (shape.slice_ptr != m.slice_ptr || shape.cols != m.cols || slots.size() != m.n_elms())
+    return fail(ISPM_ERR_INVALID, "the CSR pattern does not produce this matrix's structure");
+  pos.assign(nnz, 0u);
+  for (size_t p = 0; p < slots.size(); p++)
+    if (slots[p] > 0)
+      pos[slots[p] - 1] = (unsigned)p;
+  return ISPM_OK;
+}
+
 int guess_format(int elm_dtype, int n_rows, int n_cols, const int *row_ptr, const int *cols,
                  const void *elms, int examine_ratio, int min_height, ispm_slell_params &out)
 {
@@ -651,3 +690,21 @@ unsigned long long ispm_slell_spmv_bytes(const ispm_slell *m, int effective, int
 void ispm_slell_free(ispm_slell *m) { delete m; }
 
 }  // extern "C"
+
+extern "C" int ispm_slell_value_map(const ispm_slell *m, int n_rows, const int *row_ptr,
+                                    const int *cols, unsigned *map)
+{
+  clear_error();
+  if (!m || !map)
+    return fail(ISPM_ERR_INVALID, "NULL argument");
+  std::vector<unsigned> pos;
+  try {
+    if (int st = value_map(m->m, n_rows, row_ptr, cols, pos))
+      return st;
+  } catch (const std::bad_alloc &) {
+    return fail(ISPM_ERR_NOMEM, "host allocation while mapping values");
+  }
+  if (!pos.empty())
+    memcpy(map, pos.data(), pos.size() * sizeof(unsigned));
+  return ISPM_OK;
+}

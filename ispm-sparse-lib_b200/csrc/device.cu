@@ -87,6 +87,44 @@ int DeviceSlell::update_elms(const HostSlell &h)
   return ISPM_OK;
 }
 
+// elms[map[k]] = vals[k]: new values for an unchanged sparsity pattern,
+// written straight into the device sliced-ELL array.  Padding slots are not
+// in the map and keep their zeros.
+template <class E, class V>
+__global__ void refresh_values_kernel(E *__restrict__ elms, const unsigned *__restrict__ map,
+                                      const V *__restrict__ vals, long long n)
+{
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x)
+    elms[__ldcs(map + k)] = (E)__ldcs(vals + k);
+}
+
+int refresh_values(DeviceSlell &d, const unsigned *map, const void *vals, int val_dtype,
+                   long long n, cudaStream_t s)
+{
+  if (!n)
+    return ISPM_OK;
+  const int threads = 256;
+  long long blocks = (n + threads - 1) / threads;
+  blocks = std::min<long long>(blocks, (long long)device_sm_count() * 8);
+  const bool e32 = d.meta.elm_dtype == ISPM_F32, v32 = val_dtype == ISPM_F32;
+  if (e32 && v32)
+    refresh_values_kernel<float, float><<<blocks, threads, 0, s>>>((float *)d.elms, map,
+                                                                   (const float *)vals, n);
+  else if (e32)
+    refresh_values_kernel<float, double><<<blocks, threads, 0, s>>>((float *)d.elms, map,
+                                                                    (const double *)vals, n);
+  else if (v32)
+    refresh_values_kernel<double, float><<<blocks, threads, 0, s>>>((double *)d.elms, map,
+                                                                    (const float *)vals, n);
+  else
+    refresh_values_kernel<double, double><<<blocks, threads, 0, s>>>((double *)d.elms, map,
+                                                                     (const double *)vals, n);
+  cudaError_t e = cudaPeekAtLastError();
+  return e == cudaSuccess ? ISPM_OK
+                          : fail(ISPM_ERR_CUDA, "value refresh: %s", cudaGetErrorString(e));
+}
+
 static unsigned pow2_floor(unsigned v) { return v ? 1u << ilog2(v) : 0u; }
 static unsigned pow2_ceil(unsigned v) { return v <= 1 ? 1u : 1u << (ilog2(v - 1) + 1); }
 
@@ -208,6 +246,20 @@ int ispm_dslell_get_view(const ispm_dslell *d, ispm_slell_view *view)
 }
 
 void ispm_dslell_free(ispm_dslell *d) { delete d; }
+
+int ispm_dslell_refresh_values(ispm_dslell *d, const unsigned *map, const void *vals,
+                               int val_dtype, int n_nz, void *stream)
+{
+  clear_error();
+  if (!d || (n_nz && (!map || !vals)) || n_nz < 0)
+    return fail(ISPM_ERR_INVALID, "bad arguments");
+  if (val_dtype != ISPM_F32 && val_dtype != ISPM_F64)
+    return fail(ISPM_ERR_INVALID, "val_dtype %d", val_dtype);
+  if (n_nz != d->d.meta.n_nz)
+    return fail(ISPM_ERR_INVALID, "%d values for a matrix of %d non-zeros", n_nz,
+                d->d.meta.n_nz);
+  return refresh_values(d->d, map, vals, val_dtype, n_nz, (cudaStream_t)stream);
+}
 
 int ispm_default_launch(int x_dtype, const ispm_slell_view *m, ispm_launch_params *out)
 {

@@ -166,6 +166,10 @@ template <class in_real, class real> struct Ainv {
   const int *rp, *ci;
   const in_real *av;
   double droptol;
+  // Extended build (ispm_fastainv_sym_ex): per-row drop tolerance and a
+  // positive per-row factor on the pivot scale.  NULL in the reference build.
+  const double *row_tol = nullptr;
+  const double *row_scale = nullptr;
   RowStore<real> W;
   MergeHeap<real> heap;
   std::vector<int> u_idx, m_row;
@@ -220,8 +224,10 @@ template <class in_real, class real> struct Ainv {
     int a = 0, b = 0, m = 0;  // a walks W_i, b walks W_j (b == jl: the unit entry)
     int *mr = m_row.data();
     real *mv = m_val.data();
+    // per-row tolerance of the row being rebuilt (the extended build only)
+    const double tol = row_tol ? row_tol[i] : droptol;
     auto put = [&](int row, real v) {
-      if (std::abs(v) > droptol) {
+      if (std::abs(v) > tol) {
         mr[m] = row;
         mv[m] = v;
         m++;
@@ -345,6 +351,8 @@ template <class in_real, class real> struct Ainv {
     for (int t = 0; t < n; t++) {
       const int src = n - 1 - t;
       real scal = std::sqrt(std::abs(D[src]));
+      if (row_scale)
+        scal = (real)(scal * row_scale[src]);
       D[src] = std::copysign(scal, D[src]);
       const int *wr = W.row_of(src);
       const real *wv = W.val_of(src);
@@ -383,7 +391,8 @@ template <class in_real, class real> struct Ainv {
 template <class real>
 int fastainv_impl(int n, const int *rp, const int *ci, const double *av, ispm_progress_f progress,
                   void *pv, long long max_elts, double droptol, HostCsr &A1, HostCsr &A2,
-                  std::vector<real> &e1, std::vector<real> &e2, ispm_fastainv_stats *stats)
+                  std::vector<real> &e1, std::vector<real> &e2, ispm_fastainv_stats *stats,
+                  const double *row_tol = nullptr, const double *row_scale = nullptr)
 {
   Ainv<double, real> f;
   f.n = n;
@@ -391,6 +400,8 @@ int fastainv_impl(int n, const int *rp, const int *ci, const double *av, ispm_pr
   f.ci = ci;
   f.av = av;
   f.droptol = droptol;
+  f.row_tol = row_tol;
+  f.row_scale = row_scale;
   max_elts = std::min(max_elts, maxneed(n));
   f.W.init(n, max_elts / kChunk);
   f.run(progress, pv);
@@ -411,10 +422,13 @@ using namespace ispm;
 
 extern "C" {
 
-int ispm_fastainv_sym(int out_dtype, int n, const int *row_ptr, const int *cols,
-                      const double *elms, ispm_progress_f progress, void *v,
-                      long long max_elts, double droptol, ispm_csr **ainv1, ispm_csr **ainv2,
-                      ispm_fastainv_stats *stats)
+}  // extern "C"
+
+static int fastainv_entry(int out_dtype, int n, const int *row_ptr, const int *cols,
+                          const double *elms, ispm_progress_f progress, void *v,
+                          long long max_elts, double droptol, ispm_csr **ainv1,
+                          ispm_csr **ainv2, ispm_fastainv_stats *stats, const double *row_tol,
+                          const double *row_scale)
 {
   clear_error();
   if (!ainv1 || !ainv2)
@@ -452,10 +466,10 @@ int ispm_fastainv_sym(int out_dtype, int n, const int *row_ptr, const int *cols,
     g1->m.dtype = g2->m.dtype = out_dtype;
     if (out_dtype == ISPM_F64)
       st = fastainv_impl<double>(n, row_ptr, cols, elms, progress, v, max_elts, droptol, g1->m,
-                                 g2->m, g1->m.elms_d, g2->m.elms_d, stats);
+                                 g2->m, g1->m.elms_d, g2->m.elms_d, stats, row_tol, row_scale);
     else
       st = fastainv_impl<float>(n, row_ptr, cols, elms, progress, v, max_elts, droptol, g1->m,
-                                g2->m, g1->m.elms_f, g2->m.elms_f, stats);
+                                g2->m, g1->m.elms_f, g2->m.elms_f, stats, row_tol, row_scale);
   } catch (const std::bad_alloc &) {
     st = fail(ISPM_ERR_NOMEM, "host allocation during fastainv");
   }
@@ -467,6 +481,34 @@ int ispm_fastainv_sym(int out_dtype, int n, const int *row_ptr, const int *cols,
   *ainv1 = g1;
   *ainv2 = g2;
   return ISPM_OK;
+}
+
+extern "C" {
+
+int ispm_fastainv_sym(int out_dtype, int n, const int *row_ptr, const int *cols,
+                      const double *elms, ispm_progress_f progress, void *v,
+                      long long max_elts, double droptol, ispm_csr **ainv1, ispm_csr **ainv2,
+                      ispm_fastainv_stats *stats)
+{
+  return fastainv_entry(out_dtype, n, row_ptr, cols, elms, progress, v, max_elts, droptol,
+                        ainv1, ainv2, stats, nullptr, nullptr);
+}
+
+int ispm_fastainv_sym_ex(int out_dtype, int n, const int *row_ptr, const int *cols,
+                         const double *elms, const double *row_droptol, const double *row_scale,
+                         long long max_elts, double droptol, ispm_csr **ainv1, ispm_csr **ainv2,
+                         ispm_fastainv_stats *stats)
+{
+  if (row_droptol)
+    for (int i = 0; i < n; i++)
+      if (!(row_droptol[i] >= 0))
+        return fail(ISPM_ERR_INVALID, "row_droptol[%d] = %g", i, row_droptol[i]);
+  if (row_scale)
+    for (int i = 0; i < n; i++)
+      if (!(row_scale[i] > 0) || !std::isfinite(row_scale[i]))
+        return fail(ISPM_ERR_INVALID, "row_scale[%d] = %g", i, row_scale[i]);
+  return fastainv_entry(out_dtype, n, row_ptr, cols, elms, nullptr, nullptr, max_elts, droptol,
+                        ainv1, ainv2, stats, row_droptol, row_scale);
 }
 
 int ispm_csr_get_info(const ispm_csr *m, int *n_rows, int *n_cols, int *n_nz, int *dtype)

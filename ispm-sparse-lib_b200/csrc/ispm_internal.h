@@ -27,6 +27,7 @@ struct HostSlell {
   bool var_height = false, diags = false;
   int elm_dtype = ISPM_F64;
   unsigned min_slice_height = 0, max_slice_height = 0;
+  int min_height_used = 4;  // min_height the conversion ran with
   std::vector<unsigned> slice_ptr;
   std::vector<unsigned> cols;
   std::vector<float> elms_f;   // used when elm_dtype == ISPM_F32
@@ -46,6 +47,10 @@ int convert_csr(int elm_dtype, int n_rows, int n_cols, const int *row_ptr, const
                 int min_height, HostSlell &out);
 int guess_format(int elm_dtype, int n_rows, int n_cols, const int *row_ptr, const int *cols,
                  const void *elms, int examine_ratio, int min_height, ispm_slell_params &out);
+// pos[k] = element-array position of CSR entry k in m (m converted from a CSR
+// with this pattern).
+int value_map(const HostSlell &m, int n_rows, const int *row_ptr, const int *cols,
+              std::vector<unsigned> &pos);
 
 // Host CSR result (fastainv output).
 struct HostCsr {

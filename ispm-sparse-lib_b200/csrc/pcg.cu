@@ -39,6 +39,7 @@
 #include <vector>
 
 #include "cuda_util.cuh"
+#include "fsai.h"
 #include "sblas_impl.h"
 #include "spmv_launch.h"
 
@@ -471,6 +472,15 @@ struct DevMem {
   }
 };
 
+bool is_lower(int n, const int *rp, const int *ci)
+{
+  for (int i = 0; i < n; i++)
+    for (int e = rp[i]; e < rp[i + 1]; e++)
+      if (ci[e] > i)
+        return false;
+  return true;
+}
+
 // CSR -> reversed forms used for the factors.
 void reverse_rows(int n, const int *rp, const int *ci, const double *v, std::vector<int> &orp,
                   std::vector<int> &oci, std::vector<double> &ov)
@@ -514,7 +524,8 @@ struct Operator {
   // first 1% of rows, which misjudges the FSAI factors: their first rows are
   // the shortest).  `force` skips the search (same pattern, other precision).
   int upload(int vec_dtype, int elm_dtype, int n, const int *rp, const int *ci,
-             const double *v, const ispm_slell_params *force = nullptr)
+             const double *v, const ispm_slell_params *force = nullptr,
+             std::vector<unsigned> *value_pos = nullptr)
   {
     std::vector<float> vf;
     const void *vals = v;
@@ -555,6 +566,9 @@ struct Operator {
     clear_error();
     if (best_bytes == ~(size_t)0)
       return fail(ISPM_ERR_INVALID, "no sliced-ELL shape accepted the operator");
+    if (value_pos)  // CSR entry -> element slot, for values computed on the device
+      if (int st = value_map(best, n, rp, ci, *value_pos))
+        return st;
     if (int st = dev.upload(best))
       return st;
     lp = default_launch(vec_dtype, dev.view());
@@ -582,6 +596,7 @@ struct Solver {
   Scratch sc{};
   unsigned part_capacity = 0;  // partial slots in sc.part
   bool classic = false;        // classic PCG instead of the pipelined recurrence
+  unsigned fsai_fallbacks = 0; // GPU FSAI rows built as Jacobi rows
   double *x64 = nullptr, *r64 = nullptr, *t64 = nullptr, *b64 = nullptr;
   double *b_stage = nullptr, *x_stage = nullptr;  // device copies for host-vector solves
   void *vec[11] = {};
@@ -919,6 +934,85 @@ struct ispm_solver {
   ispm::Solver s;
 };
 
+namespace ispm {
+namespace {
+
+__global__ void scatter_kernel(double *__restrict__ out, const unsigned *__restrict__ at,
+                               const double *__restrict__ in, long long n)
+{
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x)
+    out[at[k]] = in[k];
+}
+
+template <class T> int to_device(DevMem &mem, T **d, const T *h, size_t count)
+{
+  if (int e = mem.get(d, count))
+    return e;
+  if (count)
+    ISPM_CUDA_TRY(cudaMemcpy(*d, h, count * sizeof(T), cudaMemcpyHostToDevice));
+  return ISPM_OK;
+}
+
+// The preconditioner pair from a GPU FSAI build: G on A's lower pattern and
+// its transpose, each stored in its own sliced-ELL shape; the values are
+// computed on the device and scattered into the device matrices through the
+// CSR-entry -> slot maps, so no factor value crosses the host.
+int build_fsai_on_device(Solver &S, int n, const int *rp, const int *ci, const double *v)
+{
+  std::vector<int> g_rp, g_ci, t_rp, t_ci;
+  std::vector<unsigned> t_of, pos_g, pos_t;
+  if (int e = fsai_lower_pattern(n, rp, ci, g_rp, g_ci))
+    return e;
+  fsai_transpose_pattern(n, g_rp, g_ci, t_rp, t_ci, t_of);
+  const size_t nnz_a = (size_t)rp[n], nnz_g = g_ci.size();
+  std::vector<double> zeros(nnz_g, 0.0);  // structure only; values come from the GPU
+  if (int e = S.G.upload(S.inner, S.inner, n, g_rp.data(), g_ci.data(), zeros.data(), nullptr,
+                         &pos_g))
+    return e;
+  if (int e = S.Ht.upload(S.inner, S.inner, n, t_rp.data(), t_ci.data(), zeros.data(), nullptr,
+                          &pos_t))
+    return e;
+  DevMem tmp;
+  int *a_rp_d, *a_ci_d, *g_rp_d;
+  double *a_v_d, *g_v_d, *gt_v_d;
+  unsigned *t_of_d, *pos_g_d, *pos_t_d, *fb_d;
+  if (int e = to_device(tmp, &a_rp_d, rp, (size_t)n + 1))
+    return e;
+  if (int e = to_device(tmp, &a_ci_d, ci, nnz_a))
+    return e;
+  if (int e = to_device(tmp, &a_v_d, v, nnz_a))
+    return e;
+  if (int e = to_device(tmp, &g_rp_d, g_rp.data(), g_rp.size()))
+    return e;
+  if (int e = to_device(tmp, &t_of_d, t_of.data(), nnz_g))
+    return e;
+  if (int e = to_device(tmp, &pos_g_d, pos_g.data(), nnz_g))
+    return e;
+  if (int e = to_device(tmp, &pos_t_d, pos_t.data(), nnz_g))
+    return e;
+  if (int e = tmp.get(&g_v_d, nnz_g))
+    return e;
+  if (int e = tmp.get(&gt_v_d, nnz_g))
+    return e;
+  if (int e = tmp.get(&fb_d, 1))
+    return e;
+  if (int e = fsai_build_values(n, a_rp_d, a_ci_d, a_v_d, g_rp_d, g_v_d, fb_d, 0))
+    return e;
+  const int blocks = grid_for((long long)nnz_g);
+  scatter_kernel<<<blocks, kThreads>>>(gt_v_d, t_of_d, g_v_d, (long long)nnz_g);
+  ISPM_CUDA_TRY(cudaPeekAtLastError());
+  if (int e = refresh_values(S.G.dev, pos_g_d, g_v_d, ISPM_F64, (long long)nnz_g, 0))
+    return e;
+  if (int e = refresh_values(S.Ht.dev, pos_t_d, gt_v_d, ISPM_F64, (long long)nnz_g, 0))
+    return e;
+  ISPM_CUDA_TRY(cudaMemcpy(&S.fsai_fallbacks, fb_d, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  return ISPM_OK;
+}
+
+}  // namespace
+}  // namespace ispm
+
 using namespace ispm;
 
 extern "C" {
@@ -936,6 +1030,7 @@ void ispm_solver_default_opts(ispm_solver_opts *o)
   o->replace_ratio_f32 = 1e-1;
   o->replace_ratio_f64 = 1e-4;
   o->variant = ISPM_PCG_AUTO;
+  o->prec = ISPM_PREC_GIVEN;
 }
 
 int ispm_solver_create(int n, const int *row_ptr, const int *cols, const double *vals,
@@ -970,13 +1065,24 @@ int ispm_solver_create(int n, const int *row_ptr, const int *cols, const double 
   else
     return fail(ISPM_ERR_INVALID, "variant %d", S.opts.variant);
   S.n = n;
-  S.have_prec = g1_rp && g2_rp;
+  if (S.opts.prec != ISPM_PREC_GIVEN && S.opts.prec != ISPM_PREC_FSAI_GPU)
+    return fail(ISPM_ERR_INVALID, "prec %d", S.opts.prec);
+  S.have_prec = S.opts.prec == ISPM_PREC_FSAI_GPU || (g1_rp && g2_rp);
   try {
     if (int e = S.Ain.upload(S.inner, S.inner, n, row_ptr, cols, vals))
       return e;
     if (int e = S.A64.upload(ISPM_F64, ISPM_F64, n, row_ptr, cols, vals, &S.Ain.fmt))
       return e;
-    if (S.have_prec) {
+    if (S.opts.prec == ISPM_PREC_FSAI_GPU) {
+      if (int e = build_fsai_on_device(S, n, row_ptr, cols, vals))
+        return e;
+    } else if (S.have_prec && is_lower(n, g1_rp, g1_ci)) {
+      // already banded (an FSAI pair G, G^T): store as given
+      if (int e = S.G.upload(S.inner, S.inner, n, g1_rp, g1_ci, g1_v))
+        return e;
+      if (int e = S.Ht.upload(S.inner, S.inner, n, g2_rp, g2_ci, g2_v))
+        return e;
+    } else if (S.have_prec) {
       std::vector<int> rp, ci;
       std::vector<double> v;
       reverse_rows(n, g1_rp, g1_ci, g1_v, rp, ci, v);

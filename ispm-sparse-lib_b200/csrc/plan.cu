@@ -89,6 +89,17 @@ struct ispm_plan {
   ispm_slell_params mparams{};
   ispm_launch_params params{};
   double tuned = 0;
+  // CSR entry -> device element slot, built on the first device refresh
+  unsigned *map = nullptr;
+  long long map_n = -1;
+  void drop_map()
+  {
+    if (map)
+      cudaFree(map);
+    map = nullptr;
+    map_n = -1;
+  }
+  ~ispm_plan() { drop_map(); }
 };
 
 using namespace ispm;
@@ -259,7 +270,35 @@ int ispm_plan_change_host_matrix(ispm_plan *p, int n_rows, int n_cols, const int
                            (int)p->mparams.H, p->mparams.V != 0, p->mparams.D != 0, 4, h->m))
     return st;
   p->host = std::move(h);
+  p->drop_map();
   return ISPM_OK;
+}
+
+int ispm_plan_refresh_values(ispm_plan *p, int n_rows, const int *row_ptr, const int *cols,
+                             const void *vals, int val_dtype, void *stream)
+{
+  clear_error();
+  if (!p || !p->host || !p->dev)
+    return fail(ISPM_ERR_INVALID, "plan lacks a host or device matrix");
+  if (!row_ptr || n_rows < 0)
+    return fail(ISPM_ERR_INVALID, "bad CSR pattern");
+  const long long nnz = row_ptr[n_rows];
+  if (!p->map || p->map_n != nnz) {
+    p->drop_map();
+    std::vector<unsigned> pos;
+    try {
+      if (int st = value_map(p->host->m, n_rows, row_ptr, cols, pos))
+        return st;
+    } catch (const std::bad_alloc &) {
+      return fail(ISPM_ERR_NOMEM, "host allocation while mapping values");
+    }
+    ISPM_CUDA_TRY(cudaMalloc(&p->map, std::max<size_t>(pos.size(), 1) * sizeof(unsigned)));
+    if (!pos.empty())
+      ISPM_CUDA_TRY(cudaMemcpy(p->map, pos.data(), pos.size() * sizeof(unsigned),
+                               cudaMemcpyHostToDevice));
+    p->map_n = nnz;
+  }
+  return refresh_values(p->dev->d, p->map, vals, val_dtype, nnz, (cudaStream_t)stream);
 }
 
 int ispm_plan_get_params(const ispm_plan *p, ispm_slell_params *mparams,

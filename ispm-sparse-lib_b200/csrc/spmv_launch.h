@@ -53,6 +53,10 @@ struct DeviceSlell {
 // B200 launch heuristic for a matrix: threads per slice and rows per thread.
 ispm_launch_params default_launch(int x_dtype, const ispm_slell_view &m);
 
+// d.elms[map[k]] = vals[k] for k < n (device arrays; vals FP32 or FP64).
+int refresh_values(DeviceSlell &d, const unsigned *map, const void *vals, int val_dtype,
+                   long long n, cudaStream_t s);
+
 }  // namespace ispm
 
 struct ispm_dslell {

@@ -569,7 +569,7 @@ class solver_opts(C.Structure):
     _fields_ = [("inner_dtype", C.c_int), ("tol", C.c_double), ("max_iters", C.c_int),
                 ("max_refinements", C.c_int), ("check_every", C.c_int),
                 ("use_graph", C.c_int), ("replace_ratio_f32", C.c_double),
-                ("replace_ratio_f64", C.c_double), ("variant", C.c_int)]
+                ("replace_ratio_f64", C.c_double), ("variant", C.c_int), ("prec", C.c_int)]
 
 
 class solve_stats(C.Structure):
@@ -620,7 +620,8 @@ class PCGSolver:
                  G2: csr_matrix | None = None, inner=np.float32, tol: float = 1e-10,
                  max_iters: int = 100000, max_refinements: int = 500,
                  check_every: int = 16, use_graph: bool = True,
-                 replace_ratio: float | None = None, variant: str = "auto"):
+                 replace_ratio: float | None = None, variant: str = "auto",
+                 prec: str = "given"):
         _declare_solver()
         L = _lib()
         o = solver_opts()
@@ -631,6 +632,7 @@ class PCGSolver:
         if replace_ratio is not None:
             o.replace_ratio_f32 = o.replace_ratio_f64 = replace_ratio
         o.variant = {"auto": 0, "pipelined": 1, "classic": 2}[variant]
+        o.prec = {"given": 0, "fsai_gpu": 1}[prec]
         if A.elms.dtype != np.float64:
             raise TypeError("the solver takes the FP64 matrix")
         self._keep = [A, G1, G2]
@@ -699,3 +701,68 @@ def default_launch_params(m, x_dtype=None) -> spmv_launch_params:
     p = spmv_launch_params()
     _check(L.ispm_default_launch(int(x_dtype), C.byref(v), C.byref(p)))
     return p
+
+
+def slell_value_map(m: slell_matrix, A: csr_matrix) -> np.ndarray:
+    """map[k] = element slot of CSR entry k of A in the sliced-ELL matrix m
+    (converted from a CSR with A's pattern)."""
+    L = _lib()
+    vp = C.c_void_p
+    L.ispm_slell_value_map.argtypes = [vp, C.c_int, vp, vp, vp]
+    L.ispm_slell_value_map.restype = C.c_int
+    out = np.zeros(max(A.n_nz, 1), np.uint32)
+    n_src = A.row_ptr.size - 1
+    _check(L.ispm_slell_value_map(m._h, n_src, _ptr(A.row_ptr), _ptr(A.cols), _ptr(out)))
+    return out[: A.n_nz]
+
+
+def plan_refresh_values(plan: "spmv_plan", A: csr_matrix, vals_dev, stream=None):
+    """Scatter new CSR values (device array, A's pattern) into the plan's device
+    matrix (ispm_plan_refresh_values)."""
+    L = _lib()
+    vp = C.c_void_p
+    L.ispm_plan_refresh_values.argtypes = [vp, C.c_int, vp, vp, vp, C.c_int, vp]
+    L.ispm_plan_refresh_values.restype = C.c_int
+    n_src = A.row_ptr.size - 1
+    _check(L.ispm_plan_refresh_values(plan._h, n_src, _ptr(A.row_ptr), _ptr(A.cols),
+                                      _ptr(vals_dev), _dtype_code(vals_dev), _stream(stream)))
+
+
+def fsai_sym_gpu(A: csr_matrix, out_dtype=np.float64, stats=None):
+    """FSAI pair built on the GPU (ispm_fsai_sym_gpu): (Ainv1, Ainv2) = (G, G^T)
+    with G lower triangular on A's lower pattern; Ainv2 Ainv1 ~ A^-1."""
+    L = _lib()
+    vp = C.c_void_p
+    L.ispm_fsai_sym_gpu.argtypes = [C.c_int, C.c_int, vp, vp, vp, C.POINTER(vp),
+                                    C.POINTER(vp), C.POINTER(C.c_uint)]
+    L.ispm_fsai_sym_gpu.restype = C.c_int
+    odt = F64 if np.dtype(out_dtype) == np.float64 else F32
+    g1, g2, fb = C.c_void_p(), C.c_void_p(), C.c_uint()
+    _check(L.ispm_fsai_sym_gpu(odt, A.n_rows, _ptr(A.row_ptr), _ptr(A.cols), _ptr(A.elms),
+                               C.byref(g1), C.byref(g2), C.byref(fb)))
+    if stats is not None:
+        stats["fallbacks"] = fb.value
+    return _csr_from_handle(g1), _csr_from_handle(g2)
+
+
+def fastainv_sym_ex(A: csr_matrix, out_dtype=np.float64, row_droptol=None, row_scale=None,
+                    max_elts: int = 8192000, droptol: float = 0.125, stats=None):
+    """fastainv_sym with per-row drop tolerances and pivot-scale factors
+    (ispm_fastainv_sym_ex).  Returns (Ainv1, Ainv2)."""
+    L = _lib()
+    vp = C.c_void_p
+    L.ispm_fastainv_sym_ex.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, vp, C.c_longlong,
+                                       C.c_double, C.POINTER(vp), C.POINTER(vp),
+                                       C.POINTER(fastainv_stats)]
+    L.ispm_fastainv_sym_ex.restype = C.c_int
+    odt = F64 if np.dtype(out_dtype) == np.float64 else F32
+    rt = None if row_droptol is None else np.ascontiguousarray(row_droptol, np.float64)
+    rs = None if row_scale is None else np.ascontiguousarray(row_scale, np.float64)
+    g1, g2 = C.c_void_p(), C.c_void_p()
+    st = fastainv_stats()
+    _check(L.ispm_fastainv_sym_ex(odt, A.n_rows, _ptr(A.row_ptr), _ptr(A.cols), _ptr(A.elms),
+                                  _ptr(rt), _ptr(rs), int(max_elts), float(droptol),
+                                  C.byref(g1), C.byref(g2), C.byref(st)))
+    if stats is not None:
+        stats.update({k: getattr(st, k) for k, _ in fastainv_stats._fields_})
+    return _csr_from_handle(g1), _csr_from_handle(g2)

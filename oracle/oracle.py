@@ -263,6 +263,40 @@ def csr_spmv_f64(row_ptr, cols, elms, x):
     return y
 
 
+def fsai_lower_f64(row_ptr, cols, elms):
+    """FSAI factor on A's lower pattern (the construction the GPU build runs):
+    row i solves A[P,P] y = e_i with P = {j <= i : a_ij != 0}, then
+    g_i = y / sqrt(y_i).  Dense per-row solves in FP64 -- small matrices only.
+    Returns (row_ptr, cols, vals) of G; rows whose local matrix is not
+    positive definite become Jacobi rows."""
+    n = len(row_ptr) - 1
+    g_rp = [0]
+    g_ci, g_v = [], []
+    # dictionary of keys for symmetric lookups
+    lookup = {}
+    for i in range(n):
+        for e in range(row_ptr[i], row_ptr[i + 1]):
+            lookup[(i, int(cols[e]))] = float(elms[e])
+    for i in range(n):
+        P = [int(c) for c in cols[row_ptr[i]:row_ptr[i + 1]] if c <= i]
+        K = len(P)
+        sub = np.array([[lookup.get((P[a], P[b]), 0.0) for b in range(K)] for a in range(K)])
+        try:
+            Lc = np.linalg.cholesky(sub)
+            e = np.zeros(K)
+            e[-1] = 1.0
+            y = np.linalg.solve(Lc.T, np.linalg.solve(Lc, e))
+            g = y / np.sqrt(y[-1])
+        except np.linalg.LinAlgError:
+            g = np.zeros(K)
+            aii = lookup[(i, i)]
+            g[-1] = 1.0 / np.sqrt(aii) if aii > 0 else 1.0
+        g_ci.extend(P)
+        g_v.extend(g)
+        g_rp.append(len(g_ci))
+    return (np.array(g_rp, np.int32), np.array(g_ci, np.int32), np.array(g_v))
+
+
 def pcg_f64(A, b, G1=None, G2=None, pipelined=False, tol=1e-10, max_it=100000, x0=None):
     """FP64 PCG on CSR triples (row_ptr, cols, elms); returns (x, iters, relres)."""
     n = len(A[0]) - 1
