@@ -369,6 +369,57 @@ int ispm_solver_solve_host(ispm_solver *s, const double *b_host, double *x_host,
 int ispm_solver_history(const ispm_solver *s, double *out, int cap);
 void ispm_solver_free(ispm_solver *s);
 
+/* ---- batched PCG: many independent SPD systems of uneven size, each with
+ *      one or more right-hand sides, advanced together (one set of launches
+ *      per iteration for all of them).  The reference has no batched path: a
+ *      caller with several systems per time step calls its primitives
+ *      (cuda/spmv/kernel-iface.h:20-74, util/cuda/sblas.h:1-25) once per
+ *      system.  Every (system, right-hand side) pair is a lane; lanes are
+ *      padded to whole 1024-row tiles and stacked in one device vector. ---- */
+
+#define ISPM_PREC_NONE 2 /* batched solver: no preconditioner */
+
+typedef struct ispm_batch ispm_batch;
+
+/* System k: n_rows[k] x n_rows[k] SPD CSR in FP64 (host arrays row_ptr[k],
+ * cols[k], vals[k]) with n_rhs[k] >= 1 right-hand sides.  opts (NULL: the
+ * solver defaults with prec = ISPM_PREC_FSAI_GPU and replace_ratio_f32 =
+ * 1e-3): inner_dtype, tol, max_iters (per lane), max_refinements (per lane),
+ * check_every (rounded up to an even count), use_graph, replace_ratio_f32 /
+ * _f64 (a lane pauses for a reliable update once its recursive residual fell
+ * by this factor), prec (ISPM_PREC_FSAI_GPU or ISPM_PREC_NONE).
+ * The iteration is classic PCG in the inner type with FP64 lane sums and an
+ * FP64 reliable update after every chunk. */
+int ispm_batch_create(int n_systems, const int *n_rows, const int *const *row_ptr,
+                      const int *const *cols, const double *const *vals, const int *n_rhs,
+                      const ispm_solver_opts *opts, ispm_batch **out);
+int ispm_batch_lanes(const ispm_batch *b);
+/* Length of the stacked device vectors. */
+long long ispm_batch_rows(const ispm_batch *b);
+/* Lane -> system, right-hand side, first stacked row, format group
+ * (any output may be NULL). */
+int ispm_batch_lane_info(const ispm_batch *b, int lane, int *system, int *rhs, long long *row0,
+                         int *group);
+/* Format groups: the sliced-ELL shape of each group's A and its lane count
+ * (writes at most cap entries; returns the group count). */
+int ispm_batch_groups(const ispm_batch *b, ispm_slell_params *a_fmt, int *lanes, int cap);
+/* Solve every lane; b and x are stacked device FP64 vectors of
+ * ispm_batch_rows() entries (lane l at its row0; padding rows of b zero).
+ * lane_stats (may be NULL): one entry per lane; total (may be NULL):
+ * maxima over the lanes, converged = all converged. */
+int ispm_batch_solve(ispm_batch *b, const double *b_dev, double *x_dev,
+                     ispm_solve_stats *lane_stats, ispm_solve_stats *total, void *stream);
+/* Host vectors: b_host[k] / x_host[k] hold system k's n_rhs[k] right-hand
+ * sides / solutions of n_rows[k] entries each, one after the other; copied
+ * in and out inside the call. */
+int ispm_batch_solve_host(ispm_batch *b, const double *const *b_host, double *const *x_host,
+                          ispm_solve_stats *lane_stats, ispm_solve_stats *total, void *stream);
+/* Kernels the last solve launched (graph replays counted per node). */
+int ispm_batch_launches(const ispm_batch *b);
+/* Rows of the stacked FSAI factor built as Jacobi rows. */
+unsigned ispm_batch_fsai_fallbacks(const ispm_batch *b);
+void ispm_batch_free(ispm_batch *b);
+
 /* ---- drop-tolerance tuner (fastainv/droptol-tuning.h:4-103) ------------ */
 typedef struct ispm_droptol_tuner ispm_droptol_tuner;
 ispm_droptol_tuner *ispm_droptol_tuner_create(double lo, double hi);

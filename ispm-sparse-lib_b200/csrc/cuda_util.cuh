@@ -79,6 +79,25 @@ template <int N, class T> __device__ __forceinline__ void st_vec(T *p, const T (
   }
 }
 
+// Block-wide FP64 sum; valid in thread 0.  blockDim.x <= 1024.
+__device__ __forceinline__ double block_sum_f64(double v)
+{
+  __shared__ double sh[32];
+  for (int off = 16; off > 0; off >>= 1)
+    v += __shfl_down_sync(0xffffffffu, v, off);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0)
+    sh[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    v = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+    for (int off = 16; off > 0; off >>= 1)
+      v += __shfl_down_sync(0xffffffffu, v, off);
+  }
+  return v;
+}
+
 }  // namespace ispm
 
 #endif

@@ -1,0 +1,53 @@
+// Solver operators: a CSR matrix held on the device as sliced-ELL in the
+// shape that needs the fewest bytes among a few candidates.
+#ifndef ISPM_OPERATOR_H
+#define ISPM_OPERATOR_H
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "spmv_launch.h"
+
+namespace ispm {
+
+// Sliced-ELL shape with the fewest stored bytes (slice_ptr + cols + elms)
+// for this CSR among the reference's guess and S in {32, 64, 128} with and
+// without diagonal blocks, plus S = 64 with hblock 2.  (The guess samples
+// only the first 1% of rows, which misjudges matrices whose first rows are
+// atypical, e.g. the FSAI factors, whose first rows are the shortest.)
+// fixed_height: variable-height shapes are not candidates.  The matrix may
+// be rectangular (a band of rows of a larger matrix).
+int choose_format(int elm_dtype, int n_rows, int n_cols, const int *rp, const int *ci,
+                  const double *v, bool fixed_height, ispm_slell_params &out,
+                  size_t *out_bytes = nullptr);
+
+struct Operator {
+  DeviceSlell dev;
+  ispm_launch_params lp{};
+  ispm_slell_params fmt{};
+
+  // Convert (n x n CSR, FP64 values stored as elm_dtype) and upload in the
+  // min-bytes shape, or in `force`.  value_pos: CSR entry -> element slot,
+  // for values computed later on the device.
+  int upload(int vec_dtype, int elm_dtype, int n, const int *rp, const int *ci,
+             const double *v, const ispm_slell_params *force = nullptr,
+             std::vector<unsigned> *value_pos = nullptr, bool fixed_height = false);
+  int apply(int vdt, const void *x, void *y, cudaStream_t s, const int *skip,
+            const SpmvDot *ep = nullptr) const
+  {
+    return launch_spmv(vdt, lp, dev.view(), x, y, s, skip, ep);
+  }
+  int apply_lanes(int vdt, const void *x, void *y, cudaStream_t s, const SpmvLanes &ln) const
+  {
+    return launch_spmv_lanes(vdt, lp, dev.view(), x, y, s, ln);
+  }
+  unsigned grid() const { return spmv_grid(lp, dev.view()); }
+  unsigned cta_rows() const { return spmv_cta_rows(lp, dev.view()); }
+  // Bytes of the stored matrix (slice_ptr + cols + elms).
+  size_t bytes() const;
+};
+
+}  // namespace ispm
+
+#endif

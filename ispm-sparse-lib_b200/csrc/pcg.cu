@@ -40,6 +40,7 @@
 
 #include "cuda_util.cuh"
 #include "fsai.h"
+#include "operator.h"
 #include "sblas_impl.h"
 #include "spmv_launch.h"
 
@@ -513,74 +514,6 @@ void reverse_cols(int n, const int *rp, const int *ci, const double *v, std::vec
     }
   }
 }
-
-struct Operator {
-  DeviceSlell dev;
-  ispm_launch_params lp{};
-  ispm_slell_params fmt{};
-
-  // Store the operator in the sliced-ELL shape with the fewest bytes among
-  // the reference's guess and a few fixed shapes (the guess samples only the
-  // first 1% of rows, which misjudges the FSAI factors: their first rows are
-  // the shortest).  `force` skips the search (same pattern, other precision).
-  int upload(int vec_dtype, int elm_dtype, int n, const int *rp, const int *ci,
-             const double *v, const ispm_slell_params *force = nullptr,
-             std::vector<unsigned> *value_pos = nullptr)
-  {
-    std::vector<float> vf;
-    const void *vals = v;
-    if (elm_dtype == ISPM_F32) {
-      vf.resize(rp[n]);
-      for (int k = 0; k < rp[n]; k++)
-        vf[k] = (float)v[k];
-      vals = vf.data();
-    }
-    std::vector<ispm_slell_params> cands;
-    if (force) {
-      cands.push_back(*force);
-    } else {
-      ispm_slell_params g;
-      if (int st = guess_format(elm_dtype, n, n, rp, ci, vals, 1, 4, g))
-        return st;
-      cands.push_back(g);
-      for (unsigned S : {32u, 64u, 128u})
-        for (unsigned D : {1u, 0u})
-          cands.push_back(ispm_slell_params{S, 1, 0, D});
-      cands.push_back(ispm_slell_params{64, 2, 0, 0});
-    }
-    const size_t esz = elm_dtype == ISPM_F32 ? 4 : 8;
-    HostSlell best;
-    size_t best_bytes = ~(size_t)0;
-    for (const ispm_slell_params &c : cands) {
-      HostSlell h;
-      if (convert_csr(elm_dtype, n, n, rp, ci, vals, (int)c.S, (int)c.H, c.V != 0, c.D != 0, 4,
-                      h))
-        continue;
-      const size_t bytes = 4 * h.slice_ptr.size() + 4 * h.cols.size() + esz * h.n_elms();
-      if (bytes < best_bytes) {
-        best_bytes = bytes;
-        best = std::move(h);
-        fmt = c;
-      }
-    }
-    clear_error();
-    if (best_bytes == ~(size_t)0)
-      return fail(ISPM_ERR_INVALID, "no sliced-ELL shape accepted the operator");
-    if (value_pos)  // CSR entry -> element slot, for values computed on the device
-      if (int st = value_map(best, n, rp, ci, *value_pos))
-        return st;
-    if (int st = dev.upload(best))
-      return st;
-    lp = default_launch(vec_dtype, dev.view());
-    return ISPM_OK;
-  }
-  int apply(int vdt, const void *x, void *y, cudaStream_t s, const int *skip,
-            const SpmvDot *ep = nullptr) const
-  {
-    return launch_spmv(vdt, lp, dev.view(), x, y, s, skip, ep);
-  }
-  unsigned grid() const { return spmv_grid(lp, dev.view()); }
-};
 
 }  // namespace
 

@@ -42,26 +42,8 @@ template <class T, class E> struct SpmvArgs {
   int x_al16;         // x 16-byte aligned (diagonal-window vector loads)
   const int *skip;    // optional device flag: nonzero -> the launch does nothing
   SpmvDot ep;         // optional fused epilogue: *ep.out = sum_i y_i v_i (FP64)
+  SpmvLanes ln;       // lane-segmented launches only
 };
-
-// Block-wide FP64 sum; valid in thread 0.  blockDim.x <= 1024.
-__device__ __forceinline__ double block_sum_f64(double v)
-{
-  __shared__ double sh[32];
-  for (int off = 16; off > 0; off >>= 1)
-    v += __shfl_down_sync(0xffffffffu, v, off);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  __syncthreads();
-  if (lane == 0)
-    sh[warp] = v;
-  __syncthreads();
-  if (warp == 0) {
-    v = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
-    for (int off = 16; off > 0; off >>= 1)
-      v += __shfl_down_sync(0xffffffffu, v, off);
-  }
-  return v;
-}
 
 // Finish a fused dot product: every block publishes its partial, the last
 // block to arrive adds them in block order (deterministic) and stores it.
@@ -85,6 +67,32 @@ __device__ __forceinline__ void finish_dot(double v, const SpmvDot &ep)
   if (threadIdx.x == 0) {
     *ep.out = s;
     *ep.ticket = 0u;
+  }
+}
+
+// Lane-segmented finish: the lane's last CTA to arrive adds the lane's
+// partials in CTA order (deterministic) and stores the lane's sum.
+__device__ __forceinline__ void finish_lane_dot(double v, const SpmvLanes &ln, int lane)
+{
+  __shared__ bool last;
+  v = block_sum_f64(v);
+  if (threadIdx.x == 0) {
+    ln.part[blockIdx.x] = v;
+    __threadfence();
+    last = atomicAdd(ln.ticket + lane, 1u) == (unsigned)__ldg(ln.cta_cnt + lane) - 1u;
+  }
+  __syncthreads();
+  if (!last)
+    return;
+  __threadfence();
+  const int beg = __ldg(ln.cta_beg + lane), cnt = __ldg(ln.cta_cnt + lane);
+  double s = 0.0;
+  for (int c = threadIdx.x; c < cnt; c += blockDim.x)
+    s += __ldcg(ln.part + beg + c);
+  s = block_sum_f64(s);
+  if (threadIdx.x == 0) {
+    ln.out[lane] = s;
+    ln.ticket[lane] = 0u;
   }
 }
 
@@ -169,7 +177,7 @@ __device__ __forceinline__ void load_window(const T *__restrict__ x, unsigned ba
     xv[h] = ld_x_guard(x, base + h, n);
 }
 
-template <class T, class E, int H, int W, bool VAR, bool DIAG>
+template <class T, class E, int H, int W, bool VAR, bool DIAG, bool LANES>
 __global__ void __launch_bounds__(1024) slell_spmv_kernel(SpmvArgs<T, E> a)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -181,6 +189,15 @@ __global__ void __launch_bounds__(1024) slell_spmv_kernel(SpmvArgs<T, E> a)
   const unsigned slice_in_cta = threadIdx.x >> a.log2_tps;
   const unsigned b = blockIdx.x * (blockDim.x >> a.log2_tps) + slice_in_cta;
   const bool active = b < a.n_slices;
+  int lane = 0;
+  if constexpr (LANES) {
+    // fixed slice height: the CTA's rows lie in one tile of one lane
+    static_assert(!VAR, "lane-segmented launches use a fixed slice height");
+    const unsigned row0 = blockIdx.x * (blockDim.x >> a.log2_tps) * a.slice_height;
+    lane = __ldg(a.ln.tile_lane + a.ln.tile_base + (row0 >> 10));
+    if (__ldg(a.ln.done + lane))
+      return;
+  }
 
   // Slice header (kernel.h:13-61); inactive slices walk nothing.
   unsigned e0 = 0, e1 = 0, c0 = 0, c1 = 0, cb = 0, d0 = 0, y0 = 0;
@@ -297,27 +314,30 @@ __global__ void __launch_bounds__(1024) slell_spmv_kernel(SpmvArgs<T, E> a)
   }
   if (active && t < R)
     st_vec<H, T>(a.y + y0 + t * H, acc);
-  if (a.ep.out) {
+  if (LANES ? a.ln.out != nullptr : a.ep.out != nullptr) {
     // fused y.v for the solver (the dot the next recurrence step needs)
     double dv = 0.0;
     if (active && t < R) {
-      const T *v = static_cast<const T *>(a.ep.v) + y0 + t * H;
+      const T *v = static_cast<const T *>(LANES ? a.ln.v : a.ep.v) + y0 + t * H;
 #pragma unroll
       for (int h = 0; h < H; h++)
         dv = fma((double)acc[h], (double)v[h], dv);
     }
-    finish_dot(dv, a.ep);
+    if constexpr (LANES)
+      finish_lane_dot(dv, a.ln, lane);
+    else
+      finish_dot(dv, a.ep);
   }
 }
 
-template <class T, class E, int H, int W, bool VAR, bool DIAG>
+template <class T, class E, int H, int W, bool VAR, bool DIAG, bool LANES = false>
 int launch_one(const SpmvArgs<T, E> &args, unsigned tps, cudaStream_t stream)
 {
   const unsigned block = tps >= 256 ? tps : 256;
   const unsigned spb = block / tps;
   const unsigned grid = (args.n_slices + spb - 1) / spb;
   const size_t smem = tps > 32 ? (size_t)block * H * sizeof(T) : 0;
-  slell_spmv_kernel<T, E, H, W, VAR, DIAG><<<grid, block, smem, stream>>>(args);
+  slell_spmv_kernel<T, E, H, W, VAR, DIAG, LANES><<<grid, block, smem, stream>>>(args);
   cudaError_t e = cudaPeekAtLastError();
   if (e != cudaSuccess)
     return fail(ISPM_ERR_CUDA, "SpMV launch: %s", cudaGetErrorString(e));
@@ -326,9 +346,25 @@ int launch_one(const SpmvArgs<T, E> &args, unsigned tps, cudaStream_t stream)
 
 template <class T, class E, int H>
 int launch_h(const SpmvArgs<T, E> &args, const ispm_slell_view &m, unsigned tps,
-             cudaStream_t s)
+             cudaStream_t s, bool lanes)
 {
   const bool V = m.var_height != 0, D = m.diags != 0;
+  if (lanes) {
+    if constexpr (std::is_same<T, E>::value) {
+      if (V)
+        return fail(ISPM_ERR_INVALID, "lane-segmented SpMV needs a fixed slice height");
+      switch (m.hblock) {
+      case 1:
+        return D ? launch_one<T, E, H, 1, false, true, true>(args, tps, s)
+                 : launch_one<T, E, H, 1, false, false, true>(args, tps, s);
+      case 2: return launch_one<T, E, H, 2, false, false, true>(args, tps, s);
+      case 4: return launch_one<T, E, H, 4, false, false, true>(args, tps, s);
+      }
+      return fail(ISPM_ERR_INVALID, "hblock %u", m.hblock);
+    } else {
+      return fail(ISPM_ERR_INVALID, "lane-segmented SpMV needs equal vector and element types");
+    }
+  }
   switch (m.hblock) {
   case 1:
     if (V)
@@ -348,11 +384,12 @@ int launch_h(const SpmvArgs<T, E> &args, const ispm_slell_view &m, unsigned tps,
 
 template <class T, class E>
 int launch_te(const ispm_launch_params &p, const ispm_slell_view &m, const void *x, void *y,
-              cudaStream_t s, const int *skip, const SpmvDot *ep)
+              cudaStream_t s, const int *skip, const SpmvDot *ep, const SpmvLanes *ln = nullptr)
 {
   SpmvArgs<T, E> a;
   a.skip = skip;
   a.ep = ep ? *ep : SpmvDot{};
+  a.ln = ln ? *ln : SpmvLanes{};
   if (ep && ep->out) {
     const unsigned block = p.N >= 256 ? p.N : 256;
     const unsigned grid = (m.n_slices + block / p.N - 1) / (block / p.N);
@@ -376,9 +413,9 @@ int launch_te(const ispm_launch_params &p, const ispm_slell_view &m, const void 
       !aligned(y, p.H * sizeof(T)))
     return fail(ISPM_ERR_INVALID, "matrix arrays or y not aligned to H=%u elements", p.H);
   switch (p.H) {
-  case 1: return launch_h<T, E, 1>(a, m, p.N, s);
-  case 2: return launch_h<T, E, 2>(a, m, p.N, s);
-  case 4: return launch_h<T, E, 4>(a, m, p.N, s);
+  case 1: return launch_h<T, E, 1>(a, m, p.N, s, ln != nullptr);
+  case 2: return launch_h<T, E, 2>(a, m, p.N, s, ln != nullptr);
+  case 4: return launch_h<T, E, 4>(a, m, p.N, s, ln != nullptr);
   }
   return fail(ISPM_ERR_INVALID, "H %u", p.H);
 }
@@ -421,6 +458,34 @@ int check_launch(int x_dtype, const ispm_launch_params &p, const ispm_slell_view
                   m.max_slice_height);
   }
   return ISPM_OK;
+}
+
+unsigned spmv_cta_rows(const ispm_launch_params &p, const ispm_slell_view &m)
+{
+  const unsigned block = p.N >= 256 ? p.N : 256;
+  return block / p.N * m.slice_height;
+}
+
+int launch_spmv_lanes(int x_dtype, const ispm_launch_params &p, const ispm_slell_view &m,
+                      const void *x, void *y, cudaStream_t s, const SpmvLanes &lanes)
+{
+  int st = check_launch(x_dtype, p, m);
+  if (st)
+    return st;
+  if (m.n_slices == 0)
+    return ISPM_OK;
+  if (!x || !y || !m.slice_ptr || (m.n_elms && (!m.elms)) || (m.n_cols_arr && !m.cols) ||
+      !lanes.tile_lane || !lanes.done)
+    return fail(ISPM_ERR_INVALID, "NULL pointer");
+  if (lanes.out && (!lanes.v || !lanes.part || !lanes.ticket || !lanes.cta_beg || !lanes.cta_cnt))
+    return fail(ISPM_ERR_INVALID, "lane dot without its buffers");
+  if (m.var_height || 1024u % spmv_cta_rows(p, m) != 0)
+    return fail(ISPM_ERR_INVALID, "a CTA of this launch does not fit one 1024-row tile");
+  if (x_dtype != m.elm_dtype)
+    return fail(ISPM_ERR_INVALID, "lane-segmented SpMV needs equal vector and element types");
+  if (x_dtype == ISPM_F32)
+    return launch_te<float, float>(p, m, x, y, s, nullptr, nullptr, &lanes);
+  return launch_te<double, double>(p, m, x, y, s, nullptr, nullptr, &lanes);
 }
 
 unsigned spmv_grid(const ispm_launch_params &p, const ispm_slell_view &m)

@@ -22,13 +22,37 @@ struct SpmvDot {
   unsigned part_capacity = 0;
 };
 
+// Batched solves (batch.cu): the matrix is a block-diagonal stack of lanes,
+// each padded to whole 1024-row tiles, and every CTA of the launch lies in
+// one tile.  CTAs of lanes with done[lane] != 0 return at once; with `out`
+// set, out[lane] = sum of y_i v_i over the lane's rows (FP64), finished by
+// the lane's last CTA to arrive: the CTAs of lane L are cta_beg[L] ..
+// cta_beg[L] + cta_cnt[L] - 1 of this launch, part[] holds one partial per
+// CTA and ticket[L] is a zero-initialised counter the launch leaves at zero.
+struct SpmvLanes {
+  const int *tile_lane = nullptr;  // lane of each tile (global tile index)
+  unsigned tile_base = 0;          // global tile of this launch's row 0
+  const int *done = nullptr;
+  const void *v = nullptr;
+  double *out = nullptr;
+  double *part = nullptr;
+  unsigned *ticket = nullptr;
+  const int *cta_beg = nullptr;
+  const int *cta_cnt = nullptr;
+};
+
 // Validate and launch y = A x on `s`.  `skip` (device int, may be NULL): the
 // kernel returns at once when it holds a nonzero value.
 int launch_spmv(int x_dtype, const ispm_launch_params &p, const ispm_slell_view &m,
                 const void *x, void *y, cudaStream_t s, const int *skip = nullptr,
                 const SpmvDot *ep = nullptr);
+// Lane-segmented launch (fixed slice height, T == E only).
+int launch_spmv_lanes(int x_dtype, const ispm_launch_params &p, const ispm_slell_view &m,
+                      const void *x, void *y, cudaStream_t s, const SpmvLanes &lanes);
 // CTAs a launch of matrix m with params p uses (partials a fused dot needs).
 unsigned spmv_grid(const ispm_launch_params &p, const ispm_slell_view &m);
+// Rows one CTA of such a launch covers (fixed slice height).
+unsigned spmv_cta_rows(const ispm_launch_params &p, const ispm_slell_view &m);
 
 // Device-resident sliced-ELL matrix.
 struct DeviceSlell {

@@ -766,3 +766,168 @@ def fastainv_sym_ex(A: csr_matrix, out_dtype=np.float64, row_droptol=None, row_s
     if stats is not None:
         stats.update({k: getattr(st, k) for k, _ in fastainv_stats._fields_})
     return _csr_from_handle(g1), _csr_from_handle(g2)
+
+
+# ---------------------------------------------------------------------------
+# Batched PCG: many SPD systems of uneven size, 1+ right-hand sides each
+# ---------------------------------------------------------------------------
+
+_BATCH_DECLARED = False
+
+
+def _declare_batch():
+    global _BATCH_DECLARED
+    if _BATCH_DECLARED:
+        return
+    _declare_solver()
+    L = _lib()
+    vp, i = C.c_void_p, C.c_int
+    L.ispm_batch_create.argtypes = [i, vp, vp, vp, vp, vp, C.POINTER(solver_opts),
+                                    C.POINTER(vp)]
+    L.ispm_batch_create.restype = i
+    L.ispm_batch_lanes.argtypes = [vp]
+    L.ispm_batch_lanes.restype = i
+    L.ispm_batch_rows.argtypes = [vp]
+    L.ispm_batch_rows.restype = C.c_longlong
+    L.ispm_batch_lane_info.argtypes = [vp, i, C.POINTER(i), C.POINTER(i),
+                                       C.POINTER(C.c_longlong), C.POINTER(i)]
+    L.ispm_batch_lane_info.restype = i
+    L.ispm_batch_groups.argtypes = [vp, C.POINTER(slell_params), vp, i]
+    L.ispm_batch_groups.restype = i
+    L.ispm_batch_solve.argtypes = [vp, vp, vp, vp, C.POINTER(solve_stats), vp]
+    L.ispm_batch_solve.restype = i
+    L.ispm_batch_solve_host.argtypes = [vp, vp, vp, vp, C.POINTER(solve_stats), vp]
+    L.ispm_batch_solve_host.restype = i
+    L.ispm_batch_launches.argtypes = [vp]
+    L.ispm_batch_launches.restype = i
+    L.ispm_batch_fsai_fallbacks.argtypes = [vp]
+    L.ispm_batch_fsai_fallbacks.restype = C.c_uint
+    L.ispm_batch_free.argtypes = [vp]
+    L.ispm_batch_free.restype = None
+    _BATCH_DECLARED = True
+
+
+class BatchSolver:
+    """Batched PCG over independent SPD systems (ispm_batch_*).
+
+    systems: list of FP64 csr_matrix; n_rhs: right-hand sides per system
+    (int or list).  inner: np.float32 (mixed: FP32 operators and vectors,
+    FP64 lane sums and reliable updates) or np.float64.  prec: "fsai_gpu" or
+    "none".  Every (system, rhs) pair is a lane; lanes run together and stop
+    independently."""
+
+    def __init__(self, systems, n_rhs=1, inner=np.float32, tol: float = 1e-8,
+                 max_iters: int = 100000, max_refinements: int = 500, check_every: int = 16,
+                 use_graph: bool = True, prec: str = "fsai_gpu",
+                 replace_ratio: float | None = None):
+        _declare_batch()
+        L = _lib()
+        k = len(systems)
+        if isinstance(n_rhs, int):
+            n_rhs = [n_rhs] * k
+        for A in systems:
+            if A.elms.dtype != np.float64 or A.n_rows != A.n_cols:
+                raise TypeError("the batched solver takes square FP64 matrices")
+        o = solver_opts()
+        L.ispm_solver_default_opts(C.byref(o))
+        o.inner_dtype = F64 if np.dtype(inner) == np.float64 else F32
+        o.tol, o.max_iters, o.max_refinements = tol, max_iters, max_refinements
+        o.check_every, o.use_graph = check_every, int(use_graph)
+        o.prec = {"fsai_gpu": 1, "none": 2}[prec]
+        # a lane pauses for a reliable update once its recursive residual
+        # fell by this factor (lanes advance in lockstep chunks)
+        o.replace_ratio_f32 = 1e-3 if replace_ratio is None else replace_ratio
+        if replace_ratio is not None:
+            o.replace_ratio_f64 = replace_ratio
+        rows = (C.c_int * k)(*[A.n_rows for A in systems])
+        rhs = (C.c_int * k)(*[int(r) for r in n_rhs])
+        arr = lambda f: (C.c_void_p * k)(*[_ptr(f(A)) for A in systems])
+        out = C.c_void_p()
+        _check(L.ispm_batch_create(k, rows, arr(lambda A: A.row_ptr), arr(lambda A: A.cols),
+                                   arr(lambda A: A.elms), rhs, C.byref(o), C.byref(out)))
+        self._h = out
+        self.systems = list(systems)
+        self.n_rhs = [int(r) for r in n_rhs]
+        self.opts = o
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _L is not None:
+            _L.ispm_batch_free(self._h)
+            self._h = None
+
+    @property
+    def lanes(self) -> int:
+        return int(_lib().ispm_batch_lanes(self._h))
+
+    @property
+    def rows(self) -> int:
+        return int(_lib().ispm_batch_rows(self._h))
+
+    def lane_info(self, lane: int) -> dict:
+        s, r, g = C.c_int(), C.c_int(), C.c_int()
+        r0 = C.c_longlong()
+        _check(_lib().ispm_batch_lane_info(self._h, lane, C.byref(s), C.byref(r), C.byref(r0),
+                                           C.byref(g)))
+        return {"system": s.value, "rhs": r.value, "row0": r0.value, "group": g.value}
+
+    def groups(self):
+        """[(slell_params of the group's A, lanes), ...]"""
+        n = _lib().ispm_batch_groups(self._h, None, None, 0)
+        fm = (slell_params * max(n, 1))()
+        ln = (C.c_int * max(n, 1))()
+        _lib().ispm_batch_groups(self._h, fm, ln, n)
+        return [((fm[g].S, fm[g].H, fm[g].V, fm[g].D), ln[g]) for g in range(n)]
+
+    @property
+    def launches(self) -> int:
+        return int(_lib().ispm_batch_launches(self._h))
+
+    @property
+    def fsai_fallbacks(self) -> int:
+        return int(_lib().ispm_batch_fsai_fallbacks(self._h))
+
+    def _finish(self, rc, lanes, tot):
+        if rc not in (OK, ERR_NOT_CONVERGED, ERR_BREAKDOWN):
+            _check(rc)
+        return [lanes[l].as_dict() for l in range(len(lanes))], tot.as_dict()
+
+    def solve(self, b, x, stream=None):
+        """b, x: stacked FP64 device vectors of `rows` entries.  Returns
+        (per-lane stats, totals)."""
+        lanes = (solve_stats * self.lanes)()
+        tot = solve_stats()
+        rc = _lib().ispm_batch_solve(self._h, _ptr(b), _ptr(x), lanes, C.byref(tot),
+                                     _stream(stream))
+        return self._finish(rc, lanes, tot)
+
+    def solve_host(self, bs, stream=None, out=None):
+        """bs[k]: system k's right-hand sides, shape (n_rhs[k], n) or (n,).
+        Returns (xs, per-lane stats, totals) with xs[k] shaped like bs[k]."""
+        k = len(self.systems)
+        bb = [np.ascontiguousarray(b, np.float64) for b in bs]
+        for j in range(k):
+            if bb[j].size != self.n_rhs[j] * self.systems[j].n_rows:
+                raise ValueError(f"system {j}: expected {self.n_rhs[j]} x "
+                                 f"{self.systems[j].n_rows} right-hand side values")
+        xs = [np.zeros_like(b) for b in bb] if out is None else out
+        lanes = (solve_stats * self.lanes)()
+        tot = solve_stats()
+        bp = (C.c_void_p * k)(*[_ptr(b) for b in bb])
+        xp = (C.c_void_p * k)(*[_ptr(x) for x in xs])
+        rc = _lib().ispm_batch_solve_host(self._h, bp, xp, lanes, C.byref(tot), _stream(stream))
+        st, tt = self._finish(rc, lanes, tot)
+        return xs, st, tt
+
+
+def shard_lpt(costs, world: int):
+    """Longest-processing-time assignment of independent systems to `world`
+    ranks: systems in decreasing cost order, each to the least-loaded rank
+    (ties to the lowest rank).  Returns a list of system indices per rank."""
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    load = [0.0] * world
+    out = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda j: (load[j], j))
+        out[r].append(i)
+        load[r] += costs[i]
+    return [sorted(s) for s in out]

@@ -220,3 +220,36 @@ def random_csr(n_rows: int, n_cols: int, seed: int, mean_len: float = 8.0,
     vals = np.concatenate(vals_all) if vals_all else np.zeros(0)
     return csr_matrix(n_rows, n_cols, np.array(rp, np.int32), cols.astype(np.int32),
                       vals.astype(dtype))
+
+
+def batch_systems(n_systems: int = 96, seed: int = 0, lo: int = 16, hi: int = 64,
+                  frac7: float = 0.6, sigma: float = 1.0, rhs_lo: int = 1, rhs_hi: int = 4,
+                  shift: float = 1e-3):
+    """Uneven batch of independent SPD systems: each a 7-point (probability
+    frac7) or 27-point box stencil with side lengths drawn uniformly from
+    lo..hi per axis, independent log-normal couplings exp(N(0, sigma^2)),
+    diagonal = row sum + shift, and rhs_lo..rhs_hi right-hand sides.
+    Returns (systems, n_rhs, dims)."""
+    rng = np.random.default_rng(seed)
+    systems, n_rhs, dims = [], [], []
+    for k in range(n_systems):
+        d = tuple(int(v) for v in rng.integers(lo, hi + 1, size=3))
+        points = 7 if rng.random() < frac7 else 27
+        r = int(rng.integers(rhs_lo, rhs_hi + 1))
+        systems.append(_box_lognormal(d, points, sigma, seed * 1000 + k, shift))
+        n_rhs.append(r)
+        dims.append(d + (points,))
+    return systems, n_rhs, dims
+
+
+def batch_rhs(systems, n_rhs, seed: int = 0):
+    """x_true ~ U(-1, 1) per (system, rhs) and b = A x_true, as arrays of
+    shape (n_rhs[k], n_k)."""
+    rng = np.random.default_rng(seed)
+    xs, bs = [], []
+    for A, r in zip(systems, n_rhs):
+        S = A.to_scipy()
+        x = rng.uniform(-1.0, 1.0, size=(r, A.n_rows))
+        xs.append(x)
+        bs.append(np.ascontiguousarray((S @ x.T).T))
+    return xs, bs
