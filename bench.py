@@ -21,6 +21,12 @@ flush is needed between steps.  Multi-GPU: every rank solves its own copy
 (replicas; the single system is not partitioned), time = max over ranks.
 
   python bench.py [--steps K] [--warmup W] [--gpus N] [--impl ours|reference]
+
+`--workload c4` times the batched solver instead: 96 independent SPD systems
+(7-point with probability 0.6, else 27-point; box sides uniform in 16..64 per
+axis; log-normal couplings, sigma 1; 1-4 right-hand sides each; seed 0) solved
+to 1e-8 together, against the same systems solved one at a time.  With
+several GPUs the systems are sharded by LPT (no data-path collective).
 """
 import argparse
 import json
@@ -55,6 +61,9 @@ def parse():
                    help="only launch the A SpMV of the workload (FP32 or FP64) --reps times "
                         "(a small program for ncu captures)")
     p.add_argument("--reps", type=int, default=5)
+    p.add_argument("--workload", choices=["c2", "c4"], default="c2",
+                   help="c2: the 128^3 27-point system (default); c4: the batch of 96 "
+                        "uneven systems")
     return p.parse_args()
 
 
@@ -249,6 +258,193 @@ def run_reference(args, rank, world):
     }), flush=True)
 
 
+# ---------------------------------------------------------------- batched (C4)
+C4_METRIC = "batched PCG time-to-1e-8 (96 uneven SPD systems, 1-4 right-hand sides each)"
+C4_WORKLOAD = ("96 box stencils (60% 7-point / 40% 27-point, sides U{16..64}, log-normal "
+               "couplings sigma 1, 1-4 RHS), tol 1e-8")
+
+
+def run_c4(args, rank, world, local):
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    import ispm
+    import ispm.gen as gen
+    import ispm.shard as shard
+    import oracle as O
+    ispm.ispm_initialize()
+    tol = 1e-8
+    t0 = time.time()
+    systems, n_rhs, dims = gen.batch_systems(96, seed=0)
+    _, bs = gen.batch_rhs(systems, n_rhs, seed=0)
+    mine = shard.my_shard(systems, n_rhs, rank, world)
+    sysm = [systems[i] for i in mine]
+    rhs = [n_rhs[i] for i in mine]
+    bm = [bs[i] for i in mine]
+    log(f"[c4] rank {rank}: {len(mine)} systems, {sum(rhs)} lanes, "
+        f"{sum(A.n_rows * r for A, r in zip(sysm, rhs))} lane rows (generated in "
+        f"{time.time() - t0:.1f}s)")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    B = ispm.BatchSolver(sysm, rhs, inner=np.float32, tol=tol)
+    torch.cuda.synchronize()
+    t_setup = time.perf_counter() - t0
+    log(f"[c4] batch setup {t_setup:.1f}s, groups {B.groups()}")
+    bh = np.zeros(B.rows)
+    lane_of = []
+    for lane in range(B.lanes):
+        info = B.lane_info(lane)
+        b = bm[info["system"]][info["rhs"]]
+        bh[info["row0"]:info["row0"] + b.size] = b
+        lane_of.append(info)
+    bd = torch.tensor(bh, device="cuda")
+    xd = torch.zeros_like(bd)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        B.solve(bd, xd, stream)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    stats = []
+    launches = 0
+    with ClockSampler(local) as clocks:
+        barrier()
+        for e0, e1 in evs:
+            e0.record(stream)
+            stats.append(B.solve(bd, xd, stream))
+            e1.record(stream)
+            launches += B.launches
+        barrier()
+    clk = clocks.summary()
+    t_batch = float(np.mean([e0.elapsed_time(e1) for e0, e1 in evs])) * 1e-3
+    lanes, tot = stats[-1]
+    if not tot["converged"]:
+        raise RuntimeError(f"batched solve did not converge: {tot}")
+    # every lane's true residual, rechecked on the host in FP64
+    xh = xd.cpu().numpy()
+    worst = 0.0
+    for info in lane_of:
+        A = sysm[info["system"]]
+        b = bm[info["system"]][info["rhs"]]
+        x = xh[info["row0"]:info["row0"] + A.n_rows]
+        worst = max(worst, float(np.linalg.norm(b - oracle_spmv(A, x)) / np.linalg.norm(b)))
+    its = [l["iterations"] for l in lanes]
+
+    # end to end through the public API: host right-hand sides in, host
+    # solutions out, every step
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        xs, _, tt = B.solve_host(bm)
+    barrier()
+    e2e = (time.perf_counter() - t0) / args.steps
+
+    # the same systems one at a time (what a caller of the single-system
+    # solver does), same method; and plain FP64 pipelined FSAI-PCG
+    def sequential(inner, variant):
+        solvers = [ispm.PCGSolver(A, inner=inner, tol=tol, prec="fsai_gpu", variant=variant)
+                   for A in sysm]
+        vecs = []
+        for S, A, bb in zip(solvers, sysm, bm):
+            for b in bb:
+                v = torch.zeros(S.rows, dtype=torch.float64, device="cuda")
+                v[:A.n_rows] = torch.from_numpy(b).cuda()
+                vecs.append((S, v, torch.zeros_like(v)))
+        for S, v, x in vecs:  # warm-up: one solve per right-hand side
+            S.solve(v, x, stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        e0.record(stream)
+        n_it = 0
+        for S, v, x in vecs:
+            st = S.solve(v, x, stream)
+            if not st["converged"]:
+                raise RuntimeError(f"sequential solve did not converge: {st}")
+            n_it += st["iterations"]
+        e1.record(stream)
+        barrier()
+        return e0.elapsed_time(e1) * 1e-3, n_it
+
+    t_seq_mixed, it_seq_mixed = sequential(np.float32, "auto")
+    t_seq_plain, it_seq_plain = sequential(np.float64, "pipelined")
+
+    if world > 1:
+        tt_ = torch.tensor([t_batch, e2e, t_seq_mixed, t_seq_plain], dtype=torch.float64,
+                           device="cuda")
+        dist.all_reduce(tt_, op=dist.ReduceOp.MAX)
+        t_batch, e2e, t_seq_mixed, t_seq_plain = tt_.tolist()
+        gathered = [None] * world
+        dist.all_gather_object(gathered, {"its": its, "worst": worst})
+        its = [i for g in gathered for i in g["its"]]
+        worst = max(g["worst"] for g in gathered)
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        # host FP64 PCG with the reference's fastainv pair on the two
+        # smallest systems, a bounded number of iterations, scaled by
+        # non-zeros x iterations to the whole batch
+        order = sorted(range(len(sysm)), key=lambda i: sysm[i].n_nz)[:2]
+        t_it, nnz_s = 0.0, 0
+        for i in order:
+            A = sysm[i]
+            G1, G2 = ispm.fastainv_sym(A, np.float64, None, 2_000_000_000, 0.01)
+            Ac = (A.row_ptr, A.cols, A.elms)
+            t0 = time.perf_counter()
+            _, it, _ = O.pcg_f64(Ac, bm[i][0], (G1.row_ptr, G1.cols, G1.elms),
+                                 (G2.row_ptr, G2.cols, G2.elms), pipelined=True, tol=1e-30,
+                                 max_it=args.cpu_sample_iters)
+            t_it += (time.perf_counter() - t0) / max(it, 1)
+            nnz_s += A.n_nz
+        per_nnz_it = t_it / nnz_s
+        work = sum(sysm[info["system"]].n_nz * lanes[l]["iterations"]
+                   for l, info in enumerate(lane_of))
+        cpu = {"value": per_nnz_it * work, "unit": "s", "cores": O.orc().orc_num_threads(),
+               "kind": "port",
+               "sample": f"{args.cpu_sample_iters} host pipelined FP64 FSAI-PCG iterations on "
+                         f"the 2 smallest systems (fastainv pair, droptol 0.01), scaled by "
+                         f"non-zeros x iterations to every lane"}
+    if rank == 0:
+        lane_rows = sum(A.n_rows * r for A, r in zip(sysm, rhs))
+        print(json.dumps({
+            "metric": C4_METRIC, "value": t_batch, "unit": "s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_batch * 1e3,
+            "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": C4_WORKLOAD, "systems": len(systems), "lanes": sum(n_rhs),
+                       "rows_rank0": lane_rows, "groups_rank0": B.groups(),
+                       "method": "batched classic PCG, FP32 operators and vectors, FP64 "
+                                 "lane sums and per-chunk reliable updates, GPU FSAI",
+                       "parallelism": f"systems sharded by LPT over {world} GPU(s)",
+                       "l2": "inputs larger than L2"},
+            "iterations_max": int(max(its)), "iterations_mean": float(np.mean(its)),
+            "true_relres_max": worst, "setup_s": t_setup,
+            "sequential_mixed": {"solve_s": t_seq_mixed, "iterations": it_seq_mixed,
+                                 "method": "same systems one at a time, mixed PCG + GPU FSAI"},
+            "sequential_plain_fp64": {"solve_s": t_seq_plain, "iterations": it_seq_plain,
+                                      "method": "one at a time, FP64 pipelined PCG + GPU FSAI"},
+            "speedup_vs_sequential_mixed": t_seq_mixed / t_batch,
+            "speedup_vs_sequential_plain_fp64": t_seq_plain / t_batch,
+            "clocks": clk,
+            "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": 8 * B.rows,
+                    "d2h_bytes_per_step": 8 * B.rows},
+            "gpu_launches": launches,
+            "cpu_baseline": cpu,
+            "device": ispm.get_device_string(),
+        }), flush=True)
+    del B
+    if world > 1:
+        dist.destroy_process_group()
+
+
 # ---------------------------------------------------------------- our arm
 def main():
     args = parse()
@@ -259,6 +455,8 @@ def main():
         return run_reference(args, rank, world)
     if args.kernel_only:
         return kernel_only(args)
+    if args.workload == "c4":
+        return run_c4(args, rank, world, local)
 
     import torch
     import torch.distributed as dist

@@ -420,6 +420,43 @@ int ispm_batch_launches(const ispm_batch *b);
 unsigned ispm_batch_fsai_fallbacks(const ispm_batch *b);
 void ispm_batch_free(ispm_batch *b);
 
+/* ---- learned drop tolerances (replaces the tuning search of
+ *      fastainv/droptol-tuning.h:4-103 with a per-row prediction) ---------
+ * A per-row MLP 32 -> 64 -> 64 -> 2 (ReLU; BF16 weights and inputs, FP32
+ * accumulation) predicts, from ispm_row_features, the log2 drop tolerance
+ * ratio and the log rescale of each row of the approximate inverse; the
+ * caller feeds them to ispm_fastainv_sym_ex.  Trained and run on the GPU. */
+
+/* Features (32 BF16 values per row, device output, row-major) of an FP64
+ * CSR held in device memory; nx, ny: grid dimensions of a box stencil
+ * (neighbours located by offset, nx, ny >= 3), or 0, 0 (entries in column
+ * order). */
+int ispm_row_features(int n, const int *row_ptr, const int *cols, const double *vals, int nx,
+                      int ny, void *out_bf16, void *stream);
+
+typedef struct ispm_mlp ispm_mlp;
+/* Parameter count; layout: W1[64][32], b1[64], W2[64][64], b2[64], W3[2][64],
+ * b3[2] (FP32 master copy; the kernels round W1..W3 to BF16). */
+int ispm_mlp_n_params(void);
+int ispm_mlp_create(const float *init_params, ispm_mlp **out);
+int ispm_mlp_get_params(const ispm_mlp *m, float *host_out);
+/* Replace the parameters and reset the optimiser state. */
+int ispm_mlp_set_params(ispm_mlp *m, const float *host_in);
+/* out[2 * r + o] = output o of row r (device; features device BF16). */
+int ispm_mlp_forward(const ispm_mlp *m, long long n_rows, const void *feat_bf16, float *out,
+                     void *stream);
+/* Loss sum_r sum_o w_ro (y_ro - t_ro)^2 / n_rows and its gradient (kept for
+ * ispm_mlp_adam_step; copied to grad_out, host, when non-NULL).  target and
+ * weight (NULL: all ones) are device [n_rows][2] FP32.  Deterministic. */
+int ispm_mlp_loss_grad(ispm_mlp *m, long long n_rows, const void *feat_bf16,
+                       const float *target, const float *weight, float *grad_out,
+                       double *loss_out, void *stream);
+/* One Adam step on the last gradient (plus weight_decay * parameter, an L2
+ * term, added to it). */
+int ispm_mlp_adam_step(ispm_mlp *m, float lr, float beta1, float beta2, float eps,
+                       float weight_decay, void *stream);
+void ispm_mlp_free(ispm_mlp *m);
+
 /* ---- drop-tolerance tuner (fastainv/droptol-tuning.h:4-103) ------------ */
 typedef struct ispm_droptol_tuner ispm_droptol_tuner;
 ispm_droptol_tuner *ispm_droptol_tuner_create(double lo, double hi);

@@ -871,22 +871,30 @@ int Batch::build(int n_systems, const int *n_rows, const int *const *rp, const i
         return e;
     }
   }
-  // groups: systems with the same three shapes, in order of first appearance
+  // groups: systems whose A takes the same shape, in order of first
+  // appearance (every group costs one launch per SpMV of an iteration); the
+  // factor pair of a group takes the shapes of its system with the most
+  // stored entries (summed over right-hand sides)
   std::vector<int> sys_group(n_systems);
+  std::vector<long long> heaviest;
   for (int k = 0; k < n_systems; k++) {
     int gi = -1;
     for (int j = 0; j < (int)groups.size() && gi < 0; j++)
-      if (same_shape(groups[j].fmt, shape[k].a) && same_shape(groups[j].g_fmt, shape[k].g) &&
-          same_shape(groups[j].h_fmt, shape[k].h))
+      if (same_shape(groups[j].fmt, shape[k].a))
         gi = j;
     if (gi < 0) {
       gi = (int)groups.size();
       groups.emplace_back();
       groups.back().fmt = shape[k].a;
-      groups.back().g_fmt = shape[k].g;
-      groups.back().h_fmt = shape[k].h;
+      heaviest.push_back(-1);
     }
     sys_group[k] = gi;
+    const long long w = (long long)rp[k][n_rows[k]] * n_rhs[k];
+    if (w > heaviest[gi]) {
+      heaviest[gi] = w;
+      groups[gi].g_fmt = shape[k].g;
+      groups[gi].h_fmt = shape[k].h;
+    }
   }
   // lanes: grouped, then by system, then by right-hand side
   sys_lane0.assign(n_systems, 0);
