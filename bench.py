@@ -491,6 +491,20 @@ def main():
     mixed = ispm.PCGSolver(A, G1, G2, inner=np.float32, tol=args.tol)
     plain = ispm.PCGSolver(A, G1, G2, inner=np.float64, tol=args.tol)
     log(f"[setup] GPU FSAI solver {t_setup:.1f}s, AINV solvers {time.time() - t0:.1f}s")
+    # learned per-row drop tolerances (the trained network's prediction fed to
+    # fastainv_sym_ex), judged against the plain build by the gate
+    import ispm.learn as LN
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    net = LN.MLP.load()
+    l_tau, l_scale = LN.predict_row_controls(net, A, (args.grid,) * 3)
+    t_pred = time.perf_counter() - t0
+    t0 = time.time()
+    L1, L2 = ispm.fastainv_sym_ex(A, np.float64, l_tau, l_scale, 2_000_000_000, args.droptol)
+    t_lbuild = time.time() - t0
+    learned = ispm.PCGSolver(A, L1, L2, inner=np.float32, tol=args.tol)
+    log(f"[setup] learned droptols (median {np.median(l_tau):.4f}) in {t_pred:.2f}s, "
+        f"build {t_lbuild:.1f}s, nnz(G) {L1.n_nz}")
     n_pad = best.rows
     bd = torch.zeros(n_pad, dtype=torch.float64, device="cuda")
     bd[: A.n_rows] = torch.from_numpy(b).cuda()
@@ -530,9 +544,11 @@ def main():
     for _ in range(max(1, min(args.warmup, 2))):
         mixed.solve(bd, xd, stream)
         plain.solve(bd, xd, stream)
+        learned.solve(bd, xd, stream)
     ms_mixed, st_mixed = timed(mixed, k_side, "mixed+AINV")
     ms_plain, st_plain = timed(plain, k_side, "plain FP64+AINV")
-    del mixed
+    ms_learned, st_learned = timed(learned, k_side, "mixed+learned AINV")
+    del mixed, learned
 
     # end to end through the public API: host b in, host x out, every step
     pin_b = torch.from_numpy(b.copy()).pin_memory()
@@ -569,10 +585,13 @@ def main():
     t_best = float(np.mean(ms_best)) * 1e-3
     t_mixed = float(np.mean(ms_mixed)) * 1e-3
     t_plain = float(np.mean(ms_plain)) * 1e-3
+    t_learned = float(np.mean(ms_learned)) * 1e-3
     if world > 1:
-        tt = torch.tensor([t_best, e2e, t_mixed, t_plain], dtype=torch.float64, device="cuda")
+        tt = torch.tensor([t_best, e2e, t_mixed, t_plain, t_learned], dtype=torch.float64,
+                          device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_best, e2e, t_mixed, t_plain = tt.tolist()
+        t_best, e2e, t_mixed, t_plain, t_learned = tt.tolist()
+    it_l, it_m = st_learned[-1]["iterations"], st_mixed[-1]["iterations"]
 
     # classic FP32 iteration: A SpMV (+p.Ap), r/x update, G SpMV, G^T SpMV
     # (+r.z), new direction; each reliable update: fold, FP64 SpMV, residual,
@@ -603,6 +622,15 @@ def main():
                            "fastainv_host_s": t_ainv},
             "plain_fp64_ainv": {"solve_s": t_plain, "iterations": st_plain[-1]["iterations"],
                                 "method": "pipelined FP64 PCG, fastainv droptol 0.01"},
+            "learned_mixed_ainv": {
+                "solve_s": t_learned, "iterations": it_l, "nnz_G": L1.n_nz,
+                "droptol_median": float(np.median(l_tau)), "predict_s": t_pred,
+                "fastainv_host_s": t_lbuild,
+                "gate_accepted": bool(it_l < it_m and t_learned <= t_mixed),
+                "gate_rule": "accepted only if PCG iterations drop and the solve is not "
+                             "slower than with the plain build (droptol 0.01); otherwise "
+                             "the plain factor is used",
+                "faster_than_plain": bool(t_learned < t_mixed)},
             "speedup_vs_plain_fp64": t_plain / t_best,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": profile_traffic(),

@@ -34,9 +34,10 @@ extern "C" {
 #define ISPM_ERR_TIMEOUT 7        /* a bounded device-side wait ran out */
 #define ISPM_ERR_TOO_LARGE 8      /* size beyond a documented maximum */
 
-/* element / vector types */
+/* element / vector types (ISPM_BF16: solver-internal element arrays only) */
 #define ISPM_F32 0
 #define ISPM_F64 1
+#define ISPM_BF16 2
 
 const char *ispm_error_string(int status);
 /* Message of the calling thread's most recent failing call ("" if none). */
@@ -325,6 +326,11 @@ typedef struct {
                            ispm_solver_create (none if NULL); ISPM_PREC_FSAI_GPU:
                            FSAI factor on A's lower pattern built on the GPU
                            (g1, g2 ignored) */
+  int factor_bf16;      /* FP32 inner solve: keep the preconditioner factor's values
+                           in BF16 (half the bytes of each factor application; the
+                           preconditioner stays SPD, its values lose 16 mantissa
+                           bits; A, the reductions and the reliable updates are
+                           unchanged) */
 } ispm_solver_opts;
 
 #define ISPM_PREC_GIVEN 0

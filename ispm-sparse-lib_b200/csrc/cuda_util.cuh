@@ -35,10 +35,10 @@ template <int N, class V> __device__ __forceinline__ Vec<N, V> ld_stream(const V
 {
   Vec<N, V> r;
   constexpr int bytes = N * (int)sizeof(V);
-  if constexpr (bytes == 4) {
-    if constexpr (sizeof(V) == 4 && N == 1) {
-      *reinterpret_cast<unsigned *>(&r.v[0]) = __ldcs(reinterpret_cast<const unsigned *>(p));
-    }
+  if constexpr (bytes == 2) {
+    *reinterpret_cast<unsigned short *>(r.v) = __ldcs(reinterpret_cast<const unsigned short *>(p));
+  } else if constexpr (bytes == 4) {
+    *reinterpret_cast<unsigned *>(r.v) = __ldcs(reinterpret_cast<const unsigned *>(p));
   } else if constexpr (bytes == 8) {
     uint2 t = __ldcs(reinterpret_cast<const uint2 *>(p));
     *reinterpret_cast<uint2 *>(r.v) = t;

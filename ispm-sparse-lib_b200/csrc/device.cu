@@ -1,9 +1,13 @@
 // Device initialisation and device-resident sliced-ELL matrices.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <vector>
 
 #include "cuda_util.cuh"
 #include "spmv_launch.h"
@@ -27,7 +31,16 @@ int device_sm_count()
   return cached[dev];
 }
 
-static size_t elm_size(int dtype) { return dtype == ISPM_F32 ? 4 : 8; }
+static size_t elm_size(int dtype) { return dtype == ISPM_F64 ? 8 : dtype == ISPM_F32 ? 4 : 2; }
+
+// Round to BF16, nearest even (finite values).
+static uint16_t to_bf16(float f)
+{
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  u += 0x7fffu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
 
 void DeviceSlell::release()
 {
@@ -42,10 +55,14 @@ void DeviceSlell::release()
   elms = nullptr;
 }
 
-int DeviceSlell::upload(const HostSlell &h)
+int DeviceSlell::upload(const HostSlell &h, bool bf16_values)
 {
   release();
   meta = h.view();
+  if (bf16_values && h.elm_dtype != ISPM_F32)
+    return fail(ISPM_ERR_INVALID, "BF16 storage converts an FP32 element array");
+  const int store = bf16_values ? ISPM_BF16 : h.elm_dtype;
+  meta.elm_dtype = store;
   const size_t nsp = h.slice_ptr.size(), nc = h.cols.size(), ne = h.n_elms();
   // The reference zero-fills every device allocation (util/cuda/allocator.h:14-20);
   // here every byte is overwritten by the copy that follows.
@@ -61,16 +78,22 @@ int DeviceSlell::upload(const HostSlell &h)
   };
   int st;
   if ((st = alloc((void **)&slice_ptr, nsp * 4)) || (st = alloc((void **)&cols, nc * 4)) ||
-      (st = alloc(&elms, ne * elm_size(h.elm_dtype)))) {
+      (st = alloc(&elms, ne * elm_size(store)))) {
     release();
     return st;
   }
   ISPM_CUDA_TRY(cudaMemcpy(slice_ptr, h.slice_ptr.data(), nsp * 4, cudaMemcpyHostToDevice));
   if (nc)
     ISPM_CUDA_TRY(cudaMemcpy(cols, h.cols.data(), nc * 4, cudaMemcpyHostToDevice));
-  if (ne)
+  if (ne && bf16_values) {
+    std::vector<uint16_t> b(ne);
+    for (size_t k = 0; k < ne; k++)
+      b[k] = to_bf16(h.elms_f[k]);
+    ISPM_CUDA_TRY(cudaMemcpy(elms, b.data(), ne * 2, cudaMemcpyHostToDevice));
+  } else if (ne) {
     ISPM_CUDA_TRY(
         cudaMemcpy(elms, h.elms_ptr(), ne * elm_size(h.elm_dtype), cudaMemcpyHostToDevice));
+  }
   return ISPM_OK;
 }
 
@@ -99,6 +122,16 @@ __global__ void refresh_values_kernel(E *__restrict__ elms, const unsigned *__re
     elms[__ldcs(map + k)] = (E)__ldcs(vals + k);
 }
 
+template <class V>
+__global__ void refresh_bf16_kernel(__nv_bfloat16 *__restrict__ elms,
+                                    const unsigned *__restrict__ map, const V *__restrict__ vals,
+                                    long long n)
+{
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x)
+    elms[__ldcs(map + k)] = __float2bfloat16_rn((float)__ldcs(vals + k));
+}
+
 int refresh_values(DeviceSlell &d, const unsigned *map, const void *vals, int val_dtype,
                    long long n, cudaStream_t s)
 {
@@ -108,7 +141,13 @@ int refresh_values(DeviceSlell &d, const unsigned *map, const void *vals, int va
   long long blocks = (n + threads - 1) / threads;
   blocks = std::min<long long>(blocks, (long long)device_sm_count() * 8);
   const bool e32 = d.meta.elm_dtype == ISPM_F32, v32 = val_dtype == ISPM_F32;
-  if (e32 && v32)
+  if (d.meta.elm_dtype == ISPM_BF16 && v32)
+    refresh_bf16_kernel<float><<<blocks, threads, 0, s>>>((__nv_bfloat16 *)d.elms, map,
+                                                          (const float *)vals, n);
+  else if (d.meta.elm_dtype == ISPM_BF16)
+    refresh_bf16_kernel<double><<<blocks, threads, 0, s>>>((__nv_bfloat16 *)d.elms, map,
+                                                           (const double *)vals, n);
+  else if (e32 && v32)
     refresh_values_kernel<float, float><<<blocks, threads, 0, s>>>((float *)d.elms, map,
                                                                    (const float *)vals, n);
   else if (e32)
@@ -132,9 +171,10 @@ ispm_launch_params default_launch(int x_dtype, const ispm_slell_view &m)
 {
   (void)x_dtype;
   ispm_launch_params p{};
-  const unsigned esz = m.elm_dtype == ISPM_F32 ? 4 : 8;
+  const unsigned esz = m.elm_dtype == ISPM_F64 ? 8 : m.elm_dtype == ISPM_F32 ? 4 : 2;
   const unsigned hmax = m.var_height ? m.min_slice_height : m.slice_height;
-  unsigned H = 16 / esz;  // one 128-bit load of elements per thread and step
+  // one 128-bit load of elements per thread and step, at most 4 rows
+  unsigned H = std::min(16u / esz, 4u);
   while (H > 1 && H > hmax)
     H >>= 1;
   const unsigned S = m.var_height ? m.max_slice_height : m.slice_height;

@@ -71,7 +71,7 @@ int choose_format(int elm_dtype, int n_rows, int n_cols, const int *rp, const in
 
 int Operator::upload(int vec_dtype, int elm_dtype, int n, const int *rp, const int *ci,
                      const double *v, const ispm_slell_params *force,
-                     std::vector<unsigned> *value_pos, bool fixed_height)
+                     std::vector<unsigned> *value_pos, bool fixed_height, bool bf16_values)
 {
   std::vector<float> vf;
   const void *vals = typed_values(elm_dtype, v, (size_t)rp[n], vf);
@@ -102,7 +102,7 @@ int Operator::upload(int vec_dtype, int elm_dtype, int n, const int *rp, const i
   if (value_pos)
     if (int st = value_map(best, n, rp, ci, *value_pos))
       return st;
-  if (int st = dev.upload(best))
+  if (int st = dev.upload(best, bf16_values && elm_dtype == ISPM_F32))
     return st;
   lp = default_launch(vec_dtype, dev.view());
   return ISPM_OK;
@@ -111,7 +111,7 @@ int Operator::upload(int vec_dtype, int elm_dtype, int n, const int *rp, const i
 size_t Operator::bytes() const
 {
   const ispm_slell_view m = dev.view();
-  const size_t esz = m.elm_dtype == ISPM_F32 ? 4 : 8;
+  const size_t esz = m.elm_dtype == ISPM_F64 ? 8 : m.elm_dtype == ISPM_F32 ? 4 : 2;
   return 4 * (size_t)m.n_slice_ptr + 4 * (size_t)m.n_cols_arr + esz * (size_t)m.n_elms;
 }
 

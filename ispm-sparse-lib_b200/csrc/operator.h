@@ -30,9 +30,11 @@ struct Operator {
   // Convert (n x n CSR, FP64 values stored as elm_dtype) and upload in the
   // min-bytes shape, or in `force`.  value_pos: CSR entry -> element slot,
   // for values computed later on the device.
+  // bf16_values: keep the FP32 elements as BF16 on the device.
   int upload(int vec_dtype, int elm_dtype, int n, const int *rp, const int *ci,
              const double *v, const ispm_slell_params *force = nullptr,
-             std::vector<unsigned> *value_pos = nullptr, bool fixed_height = false);
+             std::vector<unsigned> *value_pos = nullptr, bool fixed_height = false,
+             bool bf16_values = false);
   int apply(int vdt, const void *x, void *y, cudaStream_t s, const int *skip,
             const SpmvDot *ep = nullptr) const
   {

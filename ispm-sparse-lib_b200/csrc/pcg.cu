@@ -900,11 +900,12 @@ int build_fsai_on_device(Solver &S, int n, const int *rp, const int *ci, const d
   fsai_transpose_pattern(n, g_rp, g_ci, t_rp, t_ci, t_of);
   const size_t nnz_a = (size_t)rp[n], nnz_g = g_ci.size();
   std::vector<double> zeros(nnz_g, 0.0);  // structure only; values come from the GPU
+  const bool bf16 = S.inner == ISPM_F32 && S.opts.factor_bf16;
   if (int e = S.G.upload(S.inner, S.inner, n, g_rp.data(), g_ci.data(), zeros.data(), nullptr,
-                         &pos_g))
+                         &pos_g, false, bf16))
     return e;
   if (int e = S.Ht.upload(S.inner, S.inner, n, t_rp.data(), t_ci.data(), zeros.data(), nullptr,
-                          &pos_t))
+                          &pos_t, false, bf16))
     return e;
   DevMem tmp;
   int *a_rp_d, *a_ci_d, *g_rp_d;
@@ -964,6 +965,7 @@ void ispm_solver_default_opts(ispm_solver_opts *o)
   o->replace_ratio_f64 = 1e-4;
   o->variant = ISPM_PCG_AUTO;
   o->prec = ISPM_PREC_GIVEN;
+  o->factor_bf16 = 0;
 }
 
 int ispm_solver_create(int n, const int *row_ptr, const int *cols, const double *vals,
@@ -1011,18 +1013,24 @@ int ispm_solver_create(int n, const int *row_ptr, const int *cols, const double 
         return e;
     } else if (S.have_prec && is_lower(n, g1_rp, g1_ci)) {
       // already banded (an FSAI pair G, G^T): store as given
-      if (int e = S.G.upload(S.inner, S.inner, n, g1_rp, g1_ci, g1_v))
+      const bool bf16 = S.inner == ISPM_F32 && S.opts.factor_bf16;
+      if (int e = S.G.upload(S.inner, S.inner, n, g1_rp, g1_ci, g1_v, nullptr, nullptr, false,
+                             bf16))
         return e;
-      if (int e = S.Ht.upload(S.inner, S.inner, n, g2_rp, g2_ci, g2_v))
+      if (int e = S.Ht.upload(S.inner, S.inner, n, g2_rp, g2_ci, g2_v, nullptr, nullptr, false,
+                              bf16))
         return e;
     } else if (S.have_prec) {
       std::vector<int> rp, ci;
       std::vector<double> v;
+      const bool bf16 = S.inner == ISPM_F32 && S.opts.factor_bf16;
       reverse_rows(n, g1_rp, g1_ci, g1_v, rp, ci, v);
-      if (int e = S.G.upload(S.inner, S.inner, n, rp.data(), ci.data(), v.data()))
+      if (int e = S.G.upload(S.inner, S.inner, n, rp.data(), ci.data(), v.data(), nullptr,
+                             nullptr, false, bf16))
         return e;
       reverse_cols(n, g2_rp, g2_ci, g2_v, rp, ci, v);
-      if (int e = S.Ht.upload(S.inner, S.inner, n, rp.data(), ci.data(), v.data()))
+      if (int e = S.Ht.upload(S.inner, S.inner, n, rp.data(), ci.data(), v.data(), nullptr,
+                              nullptr, false, bf16))
         return e;
     }
   } catch (const std::bad_alloc &) {

@@ -17,6 +17,7 @@
 //    across the warp so slices of different heights may share one) with a
 //    shared-memory step only when a slice spans several warps;
 //  * hblock columns gather W consecutive x values with one vector load.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <type_traits>
@@ -426,9 +427,10 @@ int check_launch(int x_dtype, const ispm_launch_params &p, const ispm_slell_view
 {
   const int e = m.elm_dtype;
   if (!((x_dtype == ISPM_F32 && e == ISPM_F32) || (x_dtype == ISPM_F64 && e == ISPM_F32) ||
-        (x_dtype == ISPM_F64 && e == ISPM_F64)))
+        (x_dtype == ISPM_F64 && e == ISPM_F64) || (x_dtype == ISPM_F32 && e == ISPM_BF16)))
     return fail(ISPM_ERR_INVALID, "(T, E) = (%s, %s) is not an instantiated pair",
-                x_dtype == ISPM_F64 ? "double" : "float", e == ISPM_F64 ? "double" : "float");
+                x_dtype == ISPM_F64 ? "double" : "float",
+                e == ISPM_F64 ? "double" : e == ISPM_F32 ? "float" : "bfloat16");
   if (!is_pow2(p.N) || p.N < 4 || p.N > 1024)
     return fail(ISPM_ERR_INVALID, "N = %u (power of two in [4, 1024])", p.N);
   if (p.H != 1 && p.H != 2 && p.H != 4)
@@ -511,6 +513,8 @@ int launch_spmv(int x_dtype, const ispm_launch_params &p, const ispm_slell_view 
   }
   if (!x || !y || !m.slice_ptr || (m.n_elms && (!m.elms)) || (m.n_cols_arr && !m.cols))
     return fail(ISPM_ERR_INVALID, "NULL pointer");
+  if (x_dtype == ISPM_F32 && m.elm_dtype == ISPM_BF16)
+    return launch_te<float, __nv_bfloat16>(p, m, x, y, s, skip, ep);
   if (x_dtype == ISPM_F32)
     return launch_te<float, float>(p, m, x, y, s, skip, ep);
   if (m.elm_dtype == ISPM_F32)

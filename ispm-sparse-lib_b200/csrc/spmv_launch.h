@@ -68,7 +68,8 @@ struct DeviceSlell {
     v.elms = elms;
     return v;
   }
-  int upload(const HostSlell &h);
+  // bf16_values: keep an FP32 element array as BF16 (elm_dtype ISPM_BF16)
+  int upload(const HostSlell &h, bool bf16_values = false);
   int update_elms(const HostSlell &h);
   void release();
   ~DeviceSlell() { release(); }
