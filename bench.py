@@ -27,6 +27,12 @@ flush is needed between steps.  Multi-GPU: every rank solves its own copy
 axis; log-normal couplings, sigma 1; 1-4 right-hand sides each; seed 0) solved
 to 1e-8 together, against the same systems solved one at a time.  With
 several GPUs the systems are sharded by LPT (no data-path collective).
+
+`--workload c3` times the unstructured case: a 192^3 7-point face graph with
+5% of the face pairs removed (seed 1), weights U(0.1, 10), a random symmetric
+permutation and diagonal = 1.01 x row sum (7,077,888 rows).  The SpMV runs
+with the plan's exhaustive autotune (slice height, hblock width, launch
+shape); the solve is the mixed PCG with FP64 refinement to 1e-10.
 """
 import argparse
 import json
@@ -61,9 +67,9 @@ def parse():
                    help="only launch the A SpMV of the workload (FP32 or FP64) --reps times "
                         "(a small program for ncu captures)")
     p.add_argument("--reps", type=int, default=5)
-    p.add_argument("--workload", choices=["c2", "c4"], default="c2",
-                   help="c2: the 128^3 27-point system (default); c4: the batch of 96 "
-                        "uneven systems")
+    p.add_argument("--workload", choices=["c2", "c3", "c4"], default="c2",
+                   help="c2: the 128^3 27-point system (default); c3: the 192^3 "
+                        "unstructured permuted system; c4: the batch of 96 uneven systems")
     return p.parse_args()
 
 
@@ -256,6 +262,165 @@ def run_reference(args, rank, world):
         "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "iterations": iters, "true_relres": rel, "full_solve_s": full,
     }), flush=True)
+
+
+# ---------------------------------------------------------------- unstructured (C3)
+C3_METRIC = "PCG time-to-1e-10 residual (192^3 unstructured permuted, mixed vs plain FP64); SpMV GB/s"
+C3_WORKLOAD = ("192^3 7-point face graph, 5% pairs removed (seed 1), weights U(0.1,10), "
+               "random symmetric permutation, diagonal 1.01 x row sum")
+
+
+def run_c3(args, rank, world, local):
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    import ispm
+    import ispm.gen as gen
+    import oracle as O
+    ispm.ispm_initialize()
+    t0 = time.time()
+    A = gen.unstructured(192, 0.05, 1, 0.1, 10.0, 1.01)
+    x_true = np.random.default_rng(0).uniform(-1, 1, A.n_rows)
+    b = oracle_spmv(A, x_true)
+    log(f"[c3] matrix {A.n_rows} rows {A.n_nz} nnz in {time.time() - t0:.1f}s")
+    stream = torch.cuda.current_stream()
+
+    # FP32 SpMV with the plan's exhaustive autotune
+    A32 = ispm.csr_matrix(A.n_rows, A.n_cols, A.row_ptr, A.cols, A.elms.astype(np.float32))
+    t0 = time.time()
+    plan = ispm.spmv_plan(A32, ispm.PLAN_EXHAUSTIVE, T=np.float32)
+    t_tune = time.time() - t0
+    mp, lp = plan.mparams, plan.params
+    view = plan.host_matrix.view()
+    xs = torch.rand(A.n_cols, dtype=torch.float32, device="cuda")
+    ys = torch.zeros(view.n_rows, dtype=torch.float32, device="cuda")
+    for _ in range(5):
+        plan.execute_spmv(xs, ys, stream)
+    reps = 30
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        plan.execute_spmv(xs, ys, stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_spmv = e0.elapsed_time(e1) / reps * 1e-3
+    alg = algorithmic_bytes(view, 4)
+    peak, peak_src = measured_peak()
+    log(f"[c3] plan tuned in {t_tune:.0f}s: S={mp.S} H={mp.H} V={mp.V} D={mp.D}, "
+        f"launch N={lp.N} H={lp.H}: {t_spmv * 1e6:.1f} us")
+    del plan
+
+    # the solve: mixed PCG (GPU FSAI) vs plain FP64 pipelined PCG (same factor)
+    solvers = {}
+    t0 = time.time()
+    solvers["mixed"] = ispm.PCGSolver(A, inner=np.float32, tol=args.tol, prec="fsai_gpu")
+    solvers["plain_fp64"] = ispm.PCGSolver(A, inner=np.float64, tol=args.tol, prec="fsai_gpu",
+                                           variant="pipelined")
+    t_setup = time.time() - t0
+    n_pad = solvers["mixed"].rows
+    bd = torch.zeros(n_pad, dtype=torch.float64, device="cuda")
+    bd[: A.n_rows] = torch.from_numpy(b).cuda()
+    xd = torch.zeros_like(bd)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    res = {}
+    clk = None
+    for name, S in solvers.items():
+        for _ in range(args.warmup if name == "mixed" else 1):
+            S.solve(bd, xd, stream)
+        k = args.steps if name == "mixed" else max(1, min(args.steps, 3))
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(k)]
+        sampler = ClockSampler(local) if name == "mixed" else None
+        if sampler:
+            sampler.__enter__()
+        barrier()
+        for ea, eb in evs:
+            ea.record(stream)
+            st = S.solve(bd, xd, stream)
+            eb.record(stream)
+        barrier()
+        if sampler:
+            sampler.__exit__(None, None, None)
+            clk = sampler.summary()
+        if not st["converged"]:
+            raise RuntimeError(f"c3 {name} solve did not converge: {st}")
+        x = xd[: A.n_rows].cpu().numpy()
+        rel = float(np.linalg.norm(b - oracle_spmv(A, x)) / np.linalg.norm(b))
+        res[name] = {"solve_s": float(np.mean([ea.elapsed_time(eb) for ea, eb in evs])) * 1e-3,
+                     "iterations": st["iterations"], "reliable_updates": st["refinements"],
+                     "true_relres": rel}
+    # end to end through the public API with host vectors
+    pin_b = torch.from_numpy(b.copy()).pin_memory()
+    pin_x = torch.zeros(A.n_rows, dtype=torch.float64).pin_memory()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        solvers["mixed"].solve_host(pin_b.numpy(), stream, out=pin_x.numpy())
+    barrier()
+    e2e = (time.perf_counter() - t0) / args.steps
+    t_m = res["mixed"]["solve_s"]
+    if world > 1:
+        tt = torch.tensor([t_m, e2e, t_spmv], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_m, e2e, t_spmv = tt.tolist()
+    achieved = alg / t_spmv / 1e9
+    it = res["mixed"]["iterations"]
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        # host FP64 CSR SpMV (OpenMP over the host cores), the dominant term of
+        # a host PCG iteration, scaled to the FP64 solve's iterations x 3
+        # products per iteration
+        Ac = (A.row_ptr, A.cols, A.elms)
+        t0 = time.perf_counter()
+        k = 10
+        for _ in range(k):
+            O.csr_spmv_f64(*Ac, x_true)
+        per = (time.perf_counter() - t0) / k
+        cpu = {"value": per * 3 * res["plain_fp64"]["iterations"], "unit": "s",
+               "cores": O.orc().orc_num_threads(), "kind": "port",
+               "sample": f"{k} host FP64 CSR SpMVs ({per * 1e3:.1f} ms each), scaled by 3 "
+                         f"products per iteration x {res['plain_fp64']['iterations']} "
+                         f"iterations (vector updates not counted)"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": C3_METRIC, "value": t_m, "unit": "s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_m * 1e3,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": C3_WORKLOAD, "rows": A.n_rows, "nnz": A.n_nz,
+                       "tol": args.tol, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2",
+                       "method": "mixed FP32/FP64 classic PCG, FP64 reliable updates, "
+                                 "GPU FSAI on A's lower pattern"},
+            "mixed": res["mixed"], "plain_fp64": res["plain_fp64"],
+            "speedup_vs_plain_fp64": res["plain_fp64"]["solve_s"] / t_m,
+            "setup_s": t_setup,
+            "spmv_autotune": {"S": mp.S, "hblock": mp.H, "var_height": mp.V, "diags": mp.D,
+                              "N": lp.N, "H": lp.H, "tune_s": t_tune},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "kernel": "slell_spmv_kernel<float,float> (A, FP32, autotuned)",
+                         "algorithmic_bytes": alg, "us_per_launch": t_spmv * 1e6,
+                         "peak_source": peak_src},
+            "clocks": clk,
+            "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": 8 * A.n_rows,
+                    "d2h_bytes_per_step": 8 * A.n_rows},
+            "gpu_launches": args.steps * (it * 5 + (res["mixed"]["reliable_updates"] + 1) * 7),
+            "cpu_baseline": cpu,
+            "device": ispm.get_device_string(),
+        }), flush=True)
+    solvers.clear()
+    if world > 1:
+        dist.destroy_process_group()
 
 
 # ---------------------------------------------------------------- batched (C4)
@@ -457,6 +622,8 @@ def main():
         return kernel_only(args)
     if args.workload == "c4":
         return run_c4(args, rank, world, local)
+    if args.workload == "c3":
+        return run_c3(args, rank, world, local)
 
     import torch
     import torch.distributed as dist
