@@ -55,6 +55,34 @@ template <int N, class V> __device__ __forceinline__ Vec<N, V> ld_stream(const V
   return r;
 }
 
+// Programmatic dependent launch.  A kernel launched with the programmatic
+// serialization attribute may start while its predecessor on the stream is
+// still running: pdl_wait() blocks until the predecessor has completed and
+// its writes are visible (a no-op for a kernel launched without the
+// attribute), and pdl_trigger() lets the successor be scheduled once every
+// block of this kernel has reached it (or exited).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;"); }
+
+// Launch `kernel` on `s`, with the programmatic serialization attribute when
+// pdl is set.
+template <class... KArgs, class... Args>
+cudaError_t launch_kernel(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                          cudaStream_t s, bool pdl, Args &&...args)
+{
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = pdl ? attr : nullptr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<Args &&>(args)...);
+}
+
 // Read-only-path load for the gathered vector x (kept in L1/L2).
 template <class T> __device__ __forceinline__ T ld_x(const T *x, unsigned i) { return __ldg(x + i); }
 

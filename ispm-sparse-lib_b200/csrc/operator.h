@@ -36,9 +36,9 @@ struct Operator {
              std::vector<unsigned> *value_pos = nullptr, bool fixed_height = false,
              bool bf16_values = false);
   int apply(int vdt, const void *x, void *y, cudaStream_t s, const int *skip,
-            const SpmvDot *ep = nullptr) const
+            const SpmvDot *ep = nullptr, bool pdl = false) const
   {
-    return launch_spmv(vdt, lp, dev.view(), x, y, s, skip, ep);
+    return launch_spmv(vdt, lp, dev.view(), x, y, s, skip, ep, pdl);
   }
   int apply_lanes(int vdt, const void *x, void *y, cudaStream_t s, const SpmvLanes &ln) const
   {

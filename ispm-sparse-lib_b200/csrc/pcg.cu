@@ -321,15 +321,22 @@ __device__ __forceinline__ void cg_flags(PcgState *st, double rr)
     st->done = kCap;
 }
 
-// alpha = rz / pq; d += alpha p; r -= alpha q; rr = ||r||^2
+// alpha = rz / pq; d += alpha p; r -= alpha q.
+// Without a preconditioner (noprec) also rr = ||r||^2 (= r.z) and the stop
+// test, finished in the last block.  With one, r.r comes with r.z from the
+// G^T SpMV and the stop test runs at the head of the direction step; this
+// kernel then has no reduction: alpha = rz_new / pq, and block 0 rolls the
+// scalars (rz = rz_new, fresh = 0, it += 1) -- the direction step that read
+// the old values has finished, and no block here reads them.
 template <class T>
 __global__ void __launch_bounds__(kThreads)
     cg_update_kernel(const T *__restrict__ p, const T *__restrict__ q, T *__restrict__ r,
                      T *__restrict__ d, long long n, PcgState *st, Scratch sc, int noprec)
 {
+  pdl_wait();
   if (st->done)
     return;
-  const double alpha = st->rz / st->pq;
+  const double alpha = (noprec ? st->rz : st->rz_new) / st->pq;
   if (!(alpha > 0.0) || !isfinite(alpha)) {
     if (blockIdx.x == 0 && threadIdx.x == 0)
       st->done = kBreakdown;
@@ -355,6 +362,16 @@ __global__ void __launch_bounds__(kThreads)
     reinterpret_cast<V *>(r)[i] = rv;
     reinterpret_cast<V *>(d)[i] = dv;
   }
+  pdl_trigger();
+  if (!noprec) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      st->alpha = alpha;
+      st->rz = st->rz_new;
+      st->fresh = 0;
+      st->it += 1;
+    }
+    return;
+  }
   Acc<1> tot;
   if (grid_total<1>(acc, sc, tot) && threadIdx.x == 0) {
     st->alpha = alpha;
@@ -366,14 +383,29 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// beta = rz_new / rz (0 on a fresh start); p = z + beta p; rz = rz_new
+// beta = rz_new / rz (0 on a fresh start); p = z + beta p.
+// noprec: the last block rolls rz = rz_new (the update's stop test already
+// ran).  With a preconditioner: every block first evaluates the stop test on
+// rr (from the G^T SpMV) and block 0 records it; the scalars roll in the
+// next update kernel, so no cross-block finish is needed here.
 template <class T>
 __global__ void __launch_bounds__(kThreads)
     cg_direction_kernel(const T *__restrict__ z, T *__restrict__ p, long long n, PcgState *st,
-                        Scratch sc)
+                        Scratch sc, int noprec)
 {
+  pdl_wait();
   if (st->done)
     return;
+  if (!noprec) {
+    const double rr = st->rr;
+    const bool stop = !isfinite(rr) || rr <= st->thresh2 || rr < st->ru2 * st->rr_ref ||
+                      st->it >= st->max_it;
+    if (stop) {
+      if (blockIdx.x == 0 && threadIdx.x == 0)
+        cg_flags(st, rr);
+      return;
+    }
+  }
   const bool fresh = st->fresh;
   const double rzn = st->rz_new;
   const double beta = fresh ? 0.0 : rzn / st->rz;
@@ -400,6 +432,9 @@ __global__ void __launch_bounds__(kThreads)
       reinterpret_cast<V *>(p)[i] = pv;
     }
   }
+  pdl_trigger();
+  if (!noprec)
+    return;
   Acc<1> none{{0.0}}, tot;
   if (grid_total<1>(none, sc, tot) && threadIdx.x == 0) {
     st->beta = beta;
@@ -626,16 +661,19 @@ struct Solver {
   {
     if (!have_prec)
       return ISPM_OK;
-    if (int e = G.apply(inner, vec[R], vec[TT], s, skip))
+    if (int e = G.apply(inner, vec[R], vec[TT], s, skip, nullptr, true))
       return e;
     SpmvDot ep = dot_into(vec[R], &st->rz_new);
-    return Ht.apply(inner, vec[TT], vec[Z], s, skip, &ep);
+    ep.out2 = &st->rr;  // r.r from the same pass over r (the stop test's input)
+    return Ht.apply(inner, vec[TT], vec[Z], s, skip, &ep, true);
   }
 
   template <class T> int cg_direction(cudaStream_t s)
   {
     const T *z = (const T *)(have_prec ? vec[Z] : vec[R]);
-    cg_direction_kernel<T><<<grid_for(n_pad), kThreads, 0, s>>>(z, (T *)vec[P], n_pad, st, sc);
+    ISPM_CUDA_TRY(launch_kernel(cg_direction_kernel<T>, dim3(grid_for(n_pad)), dim3(kThreads), 0,
+                                s, true, z, (T *)vec[P], (long long)n_pad, st, sc,
+                                have_prec ? 0 : 1));
     return launched("cg direction");
   }
 
@@ -643,11 +681,11 @@ struct Solver {
   {
     const int *skip = &st->done;
     SpmvDot ep = dot_into(vec[P], &st->pq);
-    if (int e = Ain.apply(inner, vec[P], vec[Q], s, skip, &ep))
+    if (int e = Ain.apply(inner, vec[P], vec[Q], s, skip, &ep, true))
       return e;
-    cg_update_kernel<T><<<grid_for(n_pad), kThreads, 0, s>>>(
-        (const T *)vec[P], (const T *)vec[Q], (T *)vec[R], (T *)vec[D], n_pad, st, sc,
-        have_prec ? 0 : 1);
+    ISPM_CUDA_TRY(launch_kernel(cg_update_kernel<T>, dim3(grid_for(n_pad)), dim3(kThreads), 0,
+                                s, true, (const T *)vec[P], (const T *)vec[Q], (T *)vec[R],
+                                (T *)vec[D], (long long)n_pad, st, sc, have_prec ? 0 : 1));
     if (int e = launched("cg update"))
       return e;
     if (int e = cg_precondition<T>(s, skip))
@@ -1048,7 +1086,8 @@ int ispm_solver_create(int n, const int *row_ptr, const int *cols, const double 
   // dot one per CTA of that SpMV
   S.part_capacity = std::max<unsigned>(
       {4u * kMaxBlocks, S.Ain.grid(), S.have_prec ? S.Ht.grid() : 0u});
-  if (int e = S.mem.get(&S.sc.part, S.part_capacity))
+  // two sums' partials for the fused r.z / r.r epilogue
+  if (int e = S.mem.get(&S.sc.part, 2 * (size_t)S.part_capacity))
     return e;
   if (int e = S.mem.get(&S.sc.ticket, 4))
     return e;

@@ -44,6 +44,7 @@ template <class T, class E> struct SpmvArgs {
   const int *skip;    // optional device flag: nonzero -> the launch does nothing
   SpmvDot ep;         // optional fused epilogue: *ep.out = sum_i y_i v_i (FP64)
   SpmvLanes ln;       // lane-segmented launches only
+  int pdl;            // launched as a programmatic dependent of the previous kernel
 };
 
 // Finish a fused dot product: every block publishes its partial, the last
@@ -67,6 +68,36 @@ __device__ __forceinline__ void finish_dot(double v, const SpmvDot &ep)
   s = block_sum_f64(s);
   if (threadIdx.x == 0) {
     *ep.out = s;
+    *ep.ticket = 0u;
+  }
+}
+
+// Same for two sums at once (partials of the second at part[part_capacity + b]).
+__device__ __forceinline__ void finish_dot2(double v, double w, const SpmvDot &ep)
+{
+  __shared__ bool last;
+  v = block_sum_f64(v);
+  w = block_sum_f64(w);
+  if (threadIdx.x == 0) {
+    ep.part[blockIdx.x] = v;
+    ep.part[ep.part_capacity + blockIdx.x] = w;
+    __threadfence();
+    last = atomicAdd(ep.ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last)
+    return;
+  __threadfence();
+  double s = 0.0, s2 = 0.0;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+    s += __ldcg(ep.part + b);
+    s2 += __ldcg(ep.part + ep.part_capacity + b);
+  }
+  s = block_sum_f64(s);
+  s2 = block_sum_f64(s2);
+  if (threadIdx.x == 0) {
+    *ep.out = s;
+    *ep.out2 = s2;
     *ep.ticket = 0u;
   }
 }
@@ -182,6 +213,7 @@ template <class T, class E, int H, int W, bool VAR, bool DIAG, bool LANES>
 __global__ void __launch_bounds__(1024) slell_spmv_kernel(SpmvArgs<T, E> a)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  pdl_wait();             // inputs of a programmatic launch are final from here
   if (a.skip && *a.skip)  // uniform: a converged solver's graph replays as no-ops
     return;
   constexpr unsigned spe = 1 + (W > 1) + (VAR ? 1 : 0) + (DIAG ? 2 : 0);
@@ -284,6 +316,7 @@ __global__ void __launch_bounds__(1024) slell_spmv_kernel(SpmvArgs<T, E> a)
     }
   }
 
+  pdl_trigger();  // the successor may be scheduled; it waits for this grid's end
   // Reduce the partial sums of the threads sharing a row (reduce.h:80-127).
   const unsigned R = sz / H;  // row groups in this slice
   const unsigned wspan = tps < 32 ? tps : 32;
@@ -317,15 +350,21 @@ __global__ void __launch_bounds__(1024) slell_spmv_kernel(SpmvArgs<T, E> a)
     st_vec<H, T>(a.y + y0 + t * H, acc);
   if (LANES ? a.ln.out != nullptr : a.ep.out != nullptr) {
     // fused y.v for the solver (the dot the next recurrence step needs)
-    double dv = 0.0;
+    double dv = 0.0, dw = 0.0;
+    const bool two = !LANES && a.ep.out2 != nullptr;
     if (active && t < R) {
       const T *v = static_cast<const T *>(LANES ? a.ln.v : a.ep.v) + y0 + t * H;
 #pragma unroll
-      for (int h = 0; h < H; h++)
+      for (int h = 0; h < H; h++) {
         dv = fma((double)acc[h], (double)v[h], dv);
+        if (two)
+          dw = fma((double)v[h], (double)v[h], dw);
+      }
     }
     if constexpr (LANES)
       finish_lane_dot(dv, a.ln, lane);
+    else if (two)
+      finish_dot2(dv, dw, a.ep);
     else
       finish_dot(dv, a.ep);
   }
@@ -338,8 +377,10 @@ int launch_one(const SpmvArgs<T, E> &args, unsigned tps, cudaStream_t stream)
   const unsigned spb = block / tps;
   const unsigned grid = (args.n_slices + spb - 1) / spb;
   const size_t smem = tps > 32 ? (size_t)block * H * sizeof(T) : 0;
-  slell_spmv_kernel<T, E, H, W, VAR, DIAG, LANES><<<grid, block, smem, stream>>>(args);
-  cudaError_t e = cudaPeekAtLastError();
+  cudaError_t e = launch_kernel(slell_spmv_kernel<T, E, H, W, VAR, DIAG, LANES>, dim3(grid),
+                                dim3(block), smem, stream, args.pdl != 0, args);
+  if (e == cudaSuccess)
+    e = cudaPeekAtLastError();
   if (e != cudaSuccess)
     return fail(ISPM_ERR_CUDA, "SpMV launch: %s", cudaGetErrorString(e));
   return ISPM_OK;
@@ -385,9 +426,11 @@ int launch_h(const SpmvArgs<T, E> &args, const ispm_slell_view &m, unsigned tps,
 
 template <class T, class E>
 int launch_te(const ispm_launch_params &p, const ispm_slell_view &m, const void *x, void *y,
-              cudaStream_t s, const int *skip, const SpmvDot *ep, const SpmvLanes *ln = nullptr)
+              cudaStream_t s, const int *skip, const SpmvDot *ep, const SpmvLanes *ln = nullptr,
+              bool pdl = false)
 {
   SpmvArgs<T, E> a;
+  a.pdl = pdl ? 1 : 0;
   a.skip = skip;
   a.ep = ep ? *ep : SpmvDot{};
   a.ln = ln ? *ln : SpmvLanes{};
@@ -498,7 +541,8 @@ unsigned spmv_grid(const ispm_launch_params &p, const ispm_slell_view &m)
 }
 
 int launch_spmv(int x_dtype, const ispm_launch_params &p, const ispm_slell_view &m,
-                const void *x, void *y, cudaStream_t s, const int *skip, const SpmvDot *ep)
+                const void *x, void *y, cudaStream_t s, const int *skip, const SpmvDot *ep,
+                bool pdl)
 {
   int st = check_launch(x_dtype, p, m);
   if (st)
@@ -514,12 +558,12 @@ int launch_spmv(int x_dtype, const ispm_launch_params &p, const ispm_slell_view 
   if (!x || !y || !m.slice_ptr || (m.n_elms && (!m.elms)) || (m.n_cols_arr && !m.cols))
     return fail(ISPM_ERR_INVALID, "NULL pointer");
   if (x_dtype == ISPM_F32 && m.elm_dtype == ISPM_BF16)
-    return launch_te<float, __nv_bfloat16>(p, m, x, y, s, skip, ep);
+    return launch_te<float, __nv_bfloat16>(p, m, x, y, s, skip, ep, nullptr, pdl);
   if (x_dtype == ISPM_F32)
-    return launch_te<float, float>(p, m, x, y, s, skip, ep);
+    return launch_te<float, float>(p, m, x, y, s, skip, ep, nullptr, pdl);
   if (m.elm_dtype == ISPM_F32)
-    return launch_te<double, float>(p, m, x, y, s, skip, ep);
-  return launch_te<double, double>(p, m, x, y, s, skip, ep);
+    return launch_te<double, float>(p, m, x, y, s, skip, ep, nullptr, pdl);
+  return launch_te<double, double>(p, m, x, y, s, skip, ep, nullptr, pdl);
 }
 
 }  // namespace ispm

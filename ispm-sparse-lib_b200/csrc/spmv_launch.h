@@ -20,6 +20,9 @@ struct SpmvDot {
   double *part = nullptr;
   unsigned *ticket = nullptr;
   unsigned part_capacity = 0;
+  // optional second sum, *out2 = sum_i v_i^2 over the same rows (read in the
+  // same pass); its partials go to part[part_capacity + CTA]
+  double *out2 = nullptr;
 };
 
 // Batched solves (batch.cu): the matrix is a block-diagonal stack of lanes,
@@ -43,9 +46,11 @@ struct SpmvLanes {
 
 // Validate and launch y = A x on `s`.  `skip` (device int, may be NULL): the
 // kernel returns at once when it holds a nonzero value.
+// pdl: launch as a programmatic dependent of the stream's previous kernel
+// (that kernel's results are read only after it completed).
 int launch_spmv(int x_dtype, const ispm_launch_params &p, const ispm_slell_view &m,
                 const void *x, void *y, cudaStream_t s, const int *skip = nullptr,
-                const SpmvDot *ep = nullptr);
+                const SpmvDot *ep = nullptr, bool pdl = false);
 // Lane-segmented launch (fixed slice height, T == E only).
 int launch_spmv_lanes(int x_dtype, const ispm_launch_params &p, const ispm_slell_view &m,
                       const void *x, void *y, cudaStream_t s, const SpmvLanes &lanes);
