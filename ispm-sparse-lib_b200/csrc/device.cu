@@ -132,6 +132,46 @@ __global__ void refresh_bf16_kernel(__nv_bfloat16 *__restrict__ elms,
     elms[__ldcs(map + k)] = __float2bfloat16_rn((float)__ldcs(vals + k));
 }
 
+template <class E, class V>
+__global__ void refresh_gather_kernel(E *__restrict__ elms, const int *__restrict__ inv,
+                                      const V *__restrict__ vals, long long n)
+{
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x) {
+    const int src = __ldcs(inv + k);
+    elms[k] = src >= 0 ? (E)__ldg(vals + src) : E(0);
+  }
+}
+
+int refresh_values_gather(DeviceSlell &d, const int *inv, const void *vals, int val_dtype,
+                          cudaStream_t s)
+{
+  const long long n = d.meta.n_elms;
+  if (!n)
+    return ISPM_OK;
+  const int threads = 256;
+  const long long blocks =
+      std::min<long long>((n + threads - 1) / threads, (long long)device_sm_count() * 16);
+  const bool e32 = d.meta.elm_dtype == ISPM_F32, v32 = val_dtype == ISPM_F32;
+  if (d.meta.elm_dtype != ISPM_F32 && d.meta.elm_dtype != ISPM_F64)
+    return fail(ISPM_ERR_INVALID, "slot-order refresh of an element type %d", d.meta.elm_dtype);
+  if (e32 && v32)
+    refresh_gather_kernel<float, float><<<blocks, threads, 0, s>>>((float *)d.elms, inv,
+                                                                   (const float *)vals, n);
+  else if (e32)
+    refresh_gather_kernel<float, double><<<blocks, threads, 0, s>>>((float *)d.elms, inv,
+                                                                    (const double *)vals, n);
+  else if (v32)
+    refresh_gather_kernel<double, float><<<blocks, threads, 0, s>>>((double *)d.elms, inv,
+                                                                    (const float *)vals, n);
+  else
+    refresh_gather_kernel<double, double><<<blocks, threads, 0, s>>>((double *)d.elms, inv,
+                                                                     (const double *)vals, n);
+  cudaError_t e = cudaPeekAtLastError();
+  return e == cudaSuccess ? ISPM_OK
+                          : fail(ISPM_ERR_CUDA, "value refresh: %s", cudaGetErrorString(e));
+}
+
 int refresh_values(DeviceSlell &d, const unsigned *map, const void *vals, int val_dtype,
                    long long n, cudaStream_t s)
 {

@@ -89,8 +89,9 @@ struct ispm_plan {
   ispm_slell_params mparams{};
   ispm_launch_params params{};
   double tuned = 0;
-  // CSR entry -> device element slot, built on the first device refresh
-  unsigned *map = nullptr;
+  // element slot -> CSR entry (-1 for padding), built on the first device
+  // refresh
+  int *map = nullptr;
   long long map_n = -1;
   void drop_map()
   {
@@ -285,20 +286,25 @@ int ispm_plan_refresh_values(ispm_plan *p, int n_rows, const int *row_ptr, const
   const long long nnz = row_ptr[n_rows];
   if (!p->map || p->map_n != nnz) {
     p->drop_map();
-    std::vector<unsigned> pos;
+    std::vector<int> inv;
     try {
+      std::vector<unsigned> pos;
       if (int st = value_map(p->host->m, n_rows, row_ptr, cols, pos))
         return st;
+      inv.assign((size_t)p->dev->d.meta.n_elms, -1);
+      for (size_t k = 0; k < pos.size(); k++)
+        inv[pos[k]] = (int)k;
     } catch (const std::bad_alloc &) {
       return fail(ISPM_ERR_NOMEM, "host allocation while mapping values");
     }
-    ISPM_CUDA_TRY(cudaMalloc(&p->map, std::max<size_t>(pos.size(), 1) * sizeof(unsigned)));
-    if (!pos.empty())
-      ISPM_CUDA_TRY(cudaMemcpy(p->map, pos.data(), pos.size() * sizeof(unsigned),
-                               cudaMemcpyHostToDevice));
+    ISPM_CUDA_TRY(cudaMalloc(&p->map, std::max<size_t>(inv.size(), 1) * sizeof(int)));
+    if (!inv.empty())
+      ISPM_CUDA_TRY(
+          cudaMemcpy(p->map, inv.data(), inv.size() * sizeof(int), cudaMemcpyHostToDevice));
     p->map_n = nnz;
   }
-  return refresh_values(p->dev->d, p->map, vals, val_dtype, nnz, (cudaStream_t)stream);
+  // slot order: coalesced writes, reads within each slice's CSR range
+  return refresh_values_gather(p->dev->d, p->map, vals, val_dtype, (cudaStream_t)stream);
 }
 
 int ispm_plan_get_params(const ispm_plan *p, ispm_slell_params *mparams,

@@ -84,6 +84,11 @@ struct DeviceSlell {
 ispm_launch_params default_launch(int x_dtype, const ispm_slell_view &m);
 
 // d.elms[map[k]] = vals[k] for k < n (device arrays; vals FP32 or FP64).
+// Same from the slot side: d.elms[s] = vals[inv[s]] for every element slot
+// s (0 where inv[s] < 0); writes are coalesced, reads stay within a slice's
+// CSR range.
+int refresh_values_gather(DeviceSlell &d, const int *inv, const void *vals, int val_dtype,
+                          cudaStream_t s);
 int refresh_values(DeviceSlell &d, const unsigned *map, const void *vals, int val_dtype,
                    long long n, cudaStream_t s);
 
