@@ -365,9 +365,16 @@ struct Lane {
 
 struct Group {
   ispm_slell_params fmt{}, g_fmt{}, h_fmt{};
-  long long row0 = 0, rows = 0;
+  long long row0 = 0, rows = 0;  // the group's lanes in the stacked vectors
   int tile0 = 0, tiles = 0;
   int lane0 = 0, lanes = 0;
+  // the group's systems, each once, in the stacked matrices
+  std::vector<int> systems, sys_tile0;
+  int mat_tiles = 0;
+  // virtual tiles (matrix tile, lane tile): system by system, tile by tile,
+  // the system's lanes one after another
+  int2 *vt = nullptr;
+  unsigned n_vt = 0;
   Operator A64, Ain, G, Ht;
 };
 
@@ -438,6 +445,9 @@ struct Batch {
     ln.tile_lane = tile_lane;
     ln.tile_base = (unsigned)g.tile0;
     ln.done = done;
+    ln.vt = g.vt;
+    ln.n_vt = g.n_vt;
+    ln.lane_tile0 = la.lane_tile0;
     return ln;
   }
 
@@ -751,33 +761,50 @@ struct Batch {
 int Batch::build_group(Group &g, const int *const *rp, const int *const *ci,
                        const double *const *v)
 {
-  const long long rows = g.rows;
-  if (rows > 0x7fffffffLL)
-    return fail(ISPM_ERR_TOO_LARGE, "a group of %lld rows exceeds the int32 CSR range", rows);
-  long long nnz = 0;
-  for (int L = g.lane0; L < g.lane0 + g.lanes; L++) {
-    const Lane &ln = lanes[L];
-    nnz += rp[ln.system][ln.n] + ((long long)ln.ntile * kTile - ln.n);
+  // the matrix stack holds each system once, tile-padded; the virtual
+  // tiles map every lane tile onto its system's matrix tile
+  long long rows = 0, nnz = 0;
+  std::vector<int2> vt;
+  g.sys_tile0.clear();
+  for (int k : g.systems) {
+    const int n_k = sys_rows[k], nt = (n_k + kTile - 1) / kTile;
+    g.sys_tile0.push_back((int)(rows / kTile));
+    rows += (long long)nt * kTile;
+    nnz += rp[k][n_k] + ((long long)nt * kTile - n_k);
   }
-  if (nnz > 0x7fffffffLL)
-    return fail(ISPM_ERR_TOO_LARGE, "a group of %lld entries exceeds the int32 CSR range", nnz);
+  if (rows > 0x7fffffffLL || nnz > 0x7fffffffLL)
+    return fail(ISPM_ERR_TOO_LARGE, "a group of %lld rows / %lld entries exceeds the int32 "
+                "CSR range", rows, nnz);
+  g.mat_tiles = (int)(rows / kTile);
+  for (size_t s_i = 0; s_i < g.systems.size(); s_i++) {
+    const int k = g.systems[s_i];
+    const int nt = (sys_rows[k] + kTile - 1) / kTile;
+    for (int t = 0; t < nt; t++)
+      for (int L = (int)sys_lane0[k]; L < (int)sys_lane0[k] + sys_rhs[k]; L++)
+        vt.push_back(make_int2(g.sys_tile0[s_i] + t, lanes[L].tile0 + t));
+  }
+  g.n_vt = (unsigned)vt.size();
+  if (g.n_vt != (unsigned)g.tiles)
+    return fail(ISPM_ERR_INVALID, "virtual tiles do not cover the group's lanes");
+  if (int e = mem.put(&g.vt, vt.data(), vt.size()))
+    return e;
   std::vector<int> srp((size_t)rows + 1), sci((size_t)nnz);
   std::vector<double> sv((size_t)nnz);
   long long at = 0, row = 0;
   srp[0] = 0;
-  for (int L = g.lane0; L < g.lane0 + g.lanes; L++) {
-    const Lane &ln = lanes[L];
-    const int *r = rp[ln.system], *c = ci[ln.system];
-    const double *x = v[ln.system];
-    const int off = (int)(ln.row0 - g.row0);
-    for (int i = 0; i < ln.n; i++, row++) {
+  for (int k : g.systems) {
+    const int *r = rp[k], *c = ci[k];
+    const double *x = v[k];
+    const int n_k = sys_rows[k], nt = (n_k + kTile - 1) / kTile;
+    const int off = (int)row;
+    for (int i = 0; i < n_k; i++, row++) {
       for (int e = r[i]; e < r[i + 1]; e++, at++) {
         sci[at] = c[e] + off;
         sv[at] = x[e];
       }
       srp[row + 1] = (int)at;
     }
-    for (int i = ln.n; i < ln.ntile * kTile; i++, row++) {  // identity padding
+    for (int i = n_k; i < nt * kTile; i++, row++) {  // identity padding
       sci[at] = off + i;
       sv[at] = 1.0;
       at++;
@@ -848,6 +875,8 @@ int Batch::build_group(Group &g, const int *const *rp, const int *const *ci,
 int Batch::build(int n_systems, const int *n_rows, const int *const *rp, const int *const *ci,
                  const double *const *v, const int *n_rhs)
 {
+  sys_rows.assign(n_rows, n_rows + n_systems);
+  sys_rhs.assign(n_rhs, n_rhs + n_systems);
   // per-system shapes (A, and the FSAI factor pair) on a band of rows
   struct Shape {
     ispm_slell_params a, g, h;
@@ -908,6 +937,7 @@ int Batch::build(int n_systems, const int *n_rows, const int *const *rp, const i
     for (int k = 0; k < n_systems; k++) {
       if (sys_group[k] != gi)
         continue;
+      g.systems.push_back(k);
       sys_lane0[k] = (long long)lanes.size();
       for (int j = 0; j < n_rhs[k]; j++) {
         Lane ln;
@@ -944,26 +974,28 @@ int Batch::build(int n_systems, const int *n_rows, const int *const *rp, const i
       tl[t] = L;
     lt0[L] = ln.tile0;
     lnt[L] = ln.ntile;
+    // a lane's partial slots: its tiles' CTAs, in tile order, after the
+    // group's earlier lanes (a launch covers the group's lane tiles)
     const unsigned per_a = kTile / g.Ain.cta_rows();
     ab[L] = (ln.tile0 - g.tile0) * (int)per_a;
     ac[L] = ln.ntile * (int)per_a;
-    cap_a = std::max(cap_a, g.Ain.grid());
+    cap_a = std::max(cap_a, (unsigned)g.tiles * per_a);
     if (have_prec) {
       const unsigned per_h = kTile / g.Ht.cta_rows();
       hb_[L] = (ln.tile0 - g.tile0) * (int)per_h;
       hc[L] = ln.ntile * (int)per_h;
-      cap_h = std::max(cap_h, g.Ht.grid());
+      cap_h = std::max(cap_h, (unsigned)g.tiles * per_h);
     }
   }
   for (const Group &g : groups) {
-    // every CTA of a lane-segmented launch lies in one tile, and the CTAs of
-    // a lane are exactly ntile * (1024 / cta_rows) consecutive ones
+    // every CTA of a lane-segmented launch lies in one tile, and the
+    // matrix stack is exactly its tiles' CTAs
     for (const Operator *op : {&g.Ain, &g.A64, &g.G, &g.Ht}) {
       if (op == &g.G && !have_prec)
         break;
       const unsigned cr = op->cta_rows();
-      if (kTile % cr || op->grid() != (unsigned)g.tiles * (kTile / cr))
-        return fail(ISPM_ERR_INVALID, "a stacked operator's CTAs do not tile its lanes");
+      if (kTile % cr || op->grid() != (unsigned)g.mat_tiles * (kTile / cr))
+        return fail(ISPM_ERR_INVALID, "a stacked operator's CTAs do not tile its systems");
     }
   }
   const size_t nl = (size_t)n_lanes;
@@ -1100,8 +1132,6 @@ int ispm_batch_create(int n_systems, const int *n_rows, const int *const *row_pt
   } catch (const std::bad_alloc &) {
     return fail(ISPM_ERR_NOMEM, "host allocation while building the batch");
   }
-  B.sys_rows.assign(n_rows, n_rows + n_systems);
-  B.sys_rhs.assign(n_rhs, n_rhs + n_systems);
   *out = h.release();
   return ISPM_OK;
 }

@@ -83,6 +83,27 @@ cudaError_t launch_kernel(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_
   return cudaLaunchKernelEx(&cfg, kernel, static_cast<Args &&>(args)...);
 }
 
+// Same widths through the read-only path with the default cache policy, for
+// matrix data that is read again soon (several lanes sharing one matrix).
+template <int N, class V> __device__ __forceinline__ Vec<N, V> ld_keep(const V *p)
+{
+  Vec<N, V> r;
+  constexpr int bytes = N * (int)sizeof(V);
+  if constexpr (bytes == 4) {
+    *reinterpret_cast<unsigned *>(r.v) = __ldg(reinterpret_cast<const unsigned *>(p));
+  } else if constexpr (bytes == 8) {
+    *reinterpret_cast<uint2 *>(r.v) = __ldg(reinterpret_cast<const uint2 *>(p));
+  } else if constexpr (bytes == 16) {
+    *reinterpret_cast<uint4 *>(r.v) = __ldg(reinterpret_cast<const uint4 *>(p));
+  } else {
+    static_assert(bytes == 32, "vector width");
+    const uint4 *q = reinterpret_cast<const uint4 *>(p);
+    reinterpret_cast<uint4 *>(r.v)[0] = __ldg(q);
+    reinterpret_cast<uint4 *>(r.v)[1] = __ldg(q + 1);
+  }
+  return r;
+}
+
 // Read-only-path load for the gathered vector x (kept in L1/L2).
 template <class T> __device__ __forceinline__ T ld_x(const T *x, unsigned i) { return __ldg(x + i); }
 

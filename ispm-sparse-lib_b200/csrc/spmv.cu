@@ -104,12 +104,13 @@ __device__ __forceinline__ void finish_dot2(double v, double w, const SpmvDot &e
 
 // Lane-segmented finish: the lane's last CTA to arrive adds the lane's
 // partials in CTA order (deterministic) and stores the lane's sum.
-__device__ __forceinline__ void finish_lane_dot(double v, const SpmvLanes &ln, int lane)
+__device__ __forceinline__ void finish_lane_dot(double v, const SpmvLanes &ln, int lane,
+                                                unsigned slot)
 {
   __shared__ bool last;
   v = block_sum_f64(v);
   if (threadIdx.x == 0) {
-    ln.part[blockIdx.x] = v;
+    ln.part[slot] = v;
     __threadfence();
     last = atomicAdd(ln.ticket + lane, 1u) == (unsigned)__ldg(ln.cta_cnt + lane) - 1u;
   }
@@ -210,7 +211,7 @@ __device__ __forceinline__ void load_window(const T *__restrict__ x, unsigned ba
 }
 
 template <class T, class E, int H, int W, bool VAR, bool DIAG, bool LANES>
-__global__ void __launch_bounds__(1024) slell_spmv_kernel(SpmvArgs<T, E> a)
+__device__ __forceinline__ void spmv_body(const SpmvArgs<T, E> &a)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   pdl_wait();             // inputs of a programmatic launch are final from here
@@ -220,17 +221,33 @@ __global__ void __launch_bounds__(1024) slell_spmv_kernel(SpmvArgs<T, E> a)
   const unsigned tps = a.tps;
   const unsigned t = threadIdx.x & (tps - 1);
   const unsigned slice_in_cta = threadIdx.x >> a.log2_tps;
-  const unsigned b = blockIdx.x * (blockDim.x >> a.log2_tps) + slice_in_cta;
-  const bool active = b < a.n_slices;
+  const unsigned spb = blockDim.x >> a.log2_tps;
+  unsigned cta = blockIdx.x;
+  const T *__restrict__ xp = a.x;
+  T *__restrict__ yp = a.y;
+  long long shift = 0;
   int lane = 0;
+  unsigned slot = 0;
   if constexpr (LANES) {
-    // fixed slice height: the CTA's rows lie in one tile of one lane
+    // fixed slice height: the CTA's rows lie in one tile; the virtual tile
+    // names the matrix tile it reads and the lane tile it serves
     static_assert(!VAR, "lane-segmented launches use a fixed slice height");
-    const unsigned row0 = blockIdx.x * (blockDim.x >> a.log2_tps) * a.slice_height;
-    lane = __ldg(a.ln.tile_lane + a.ln.tile_base + (row0 >> 10));
+    const unsigned per = 1024u / (spb * a.slice_height);
+    const unsigned vt = blockIdx.x / per, q = blockIdx.x - vt * per;
+    const int2 e = __ldg(a.ln.vt + vt);
+    lane = __ldg(a.ln.tile_lane + e.y);
     if (__ldg(a.ln.done + lane))
       return;
+    cta = (unsigned)e.x * per + q;
+    shift = ((long long)e.y - (long long)a.ln.tile_base - (long long)e.x) * 1024;
+    xp += shift;
+    yp += shift;
+    if (a.ln.out)
+      slot = (unsigned)__ldg(a.ln.cta_beg + lane) +
+             (unsigned)(e.y - __ldg(a.ln.lane_tile0 + lane)) * per + q;
   }
+  const unsigned b = cta * spb + slice_in_cta;
+  const bool active = b < a.n_slices;
 
   // Slice header (kernel.h:13-61); inactive slices walk nothing.
   unsigned e0 = 0, e1 = 0, c0 = 0, c1 = 0, cb = 0, d0 = 0, y0 = 0;
@@ -262,6 +279,14 @@ __global__ void __launch_bounds__(1024) slell_spmv_kernel(SpmvArgs<T, E> a)
     }
   }
 
+  // lanes of one system read its matrix tile one after another: keep it in
+  // L2 (default policy); a single system streams it past (evict-first)
+  auto ld_m = [](const auto *q) {
+    if constexpr (LANES)
+      return ld_keep<H>(q);
+    else
+      return ld_stream<H>(q);
+  };
   const unsigned step = tps * H;
   T acc[H];
 #pragma unroll
@@ -272,11 +297,11 @@ __global__ void __launch_bounds__(1024) slell_spmv_kernel(SpmvArgs<T, E> a)
   // ELL part with explicit columns (kernel.h:70-79).
 #pragma unroll 4
   for (; j < c1; i += step, j += step) {
-    Vec<H, unsigned> cc = ld_stream<H>(a.cols + j);
-    Vec<H, E> ee = ld_stream<H>(a.elms + i);
+    Vec<H, unsigned> cc = ld_m(a.cols + j);
+    Vec<H, E> ee = ld_m(a.elms + i);
 #pragma unroll
     for (int h = 0; h < H; h++)
-      acc[h] = fma(T(ee.v[h]), ld_x_guard(a.x, cc.v[h], a.n_cols), acc[h]);
+      acc[h] = fma(T(ee.v[h]), ld_x_guard(xp, cc.v[h], a.n_cols), acc[h]);
   }
   if constexpr (DIAG) {
     // Diagonal blocks (kernel.h:80-92): column index = diag_pos + row - sz.
@@ -287,9 +312,9 @@ __global__ void __launch_bounds__(1024) slell_spmv_kernel(SpmvArgs<T, E> a)
 #pragma unroll 4
     for (; i < e1; i += step, jj += jstep) {
       const unsigned base = __ldg(a.sp + jj) + adj;
-      Vec<H, E> ee = ld_stream<H>(a.elms + i);
+      Vec<H, E> ee = ld_m(a.elms + i);
       T xv[H];
-      load_window<T, H>(a.x, base, a.n_cols, vec_ok, xv);
+      load_window<T, H>(xp, base, a.n_cols, vec_ok, xv);
 #pragma unroll
       for (int h = 0; h < H; h++)
         acc[h] = fma(T(ee.v[h]), xv[h], acc[h]);
@@ -300,15 +325,15 @@ __global__ void __launch_bounds__(1024) slell_spmv_kernel(SpmvArgs<T, E> a)
     const bool vec_ok = a.x_vec_ok;
 #pragma unroll 2
     for (; j < cb; i += W * step, j += step) {
-      Vec<H, unsigned> cc = ld_stream<H>(a.cols + j);
+      Vec<H, unsigned> cc = ld_m(a.cols + j);
       Vec<H, E> ew[W];
 #pragma unroll
       for (int w = 0; w < W; w++)
-        ew[w] = ld_stream<H>(a.elms + i + w * sz);
+        ew[w] = ld_m(a.elms + i + w * sz);
 #pragma unroll
       for (int h = 0; h < H; h++) {
         T xw[W];
-        gather_w<T, W>(a.x, cc.v[h], a.n_cols, vec_ok, xw);
+        gather_w<T, W>(xp, cc.v[h], a.n_cols, vec_ok, xw);
 #pragma unroll
         for (int w = 0; w < W; w++)
           acc[h] = fma(T(ew[w].v[h]), xw[w], acc[h]);
@@ -347,13 +372,13 @@ __global__ void __launch_bounds__(1024) slell_spmv_kernel(SpmvArgs<T, E> a)
     }
   }
   if (active && t < R)
-    st_vec<H, T>(a.y + y0 + t * H, acc);
+    st_vec<H, T>(yp + y0 + t * H, acc);
   if (LANES ? a.ln.out != nullptr : a.ep.out != nullptr) {
     // fused y.v for the solver (the dot the next recurrence step needs)
     double dv = 0.0, dw = 0.0;
     const bool two = !LANES && a.ep.out2 != nullptr;
     if (active && t < R) {
-      const T *v = static_cast<const T *>(LANES ? a.ln.v : a.ep.v) + y0 + t * H;
+      const T *v = static_cast<const T *>(LANES ? a.ln.v : a.ep.v) + shift + y0 + t * H;
 #pragma unroll
       for (int h = 0; h < H; h++) {
         dv = fma((double)acc[h], (double)v[h], dv);
@@ -362,7 +387,7 @@ __global__ void __launch_bounds__(1024) slell_spmv_kernel(SpmvArgs<T, E> a)
       }
     }
     if constexpr (LANES)
-      finish_lane_dot(dv, a.ln, lane);
+      finish_lane_dot(dv, a.ln, lane, slot);
     else if (two)
       finish_dot2(dv, dw, a.ep);
     else
@@ -370,15 +395,37 @@ __global__ void __launch_bounds__(1024) slell_spmv_kernel(SpmvArgs<T, E> a)
   }
 }
 
+template <class T, class E, int H, int W, bool VAR, bool DIAG>
+__global__ void __launch_bounds__(1024) slell_spmv_kernel(SpmvArgs<T, E> a)
+{
+  spmv_body<T, E, H, W, VAR, DIAG, false>(a);
+}
+
+// Lane-segmented instances: bounded to two 1024-thread CTAs' registers per
+// SM (the virtual-tile set-up costs registers the single-system instances do
+// not have).
+template <class T, class E, int H, int W, bool DIAG>
+__global__ void __launch_bounds__(1024, 2) slell_spmv_lanes_kernel(SpmvArgs<T, E> a)
+{
+  spmv_body<T, E, H, W, false, DIAG, true>(a);
+}
+
 template <class T, class E, int H, int W, bool VAR, bool DIAG, bool LANES = false>
 int launch_one(const SpmvArgs<T, E> &args, unsigned tps, cudaStream_t stream)
 {
   const unsigned block = tps >= 256 ? tps : 256;
   const unsigned spb = block / tps;
-  const unsigned grid = (args.n_slices + spb - 1) / spb;
+  // lane-segmented: every virtual tile takes 1024 / (spb * S) CTAs
+  const unsigned grid = LANES ? args.ln.n_vt * (1024u / (spb * args.slice_height))
+                              : (args.n_slices + spb - 1) / spb;
   const size_t smem = tps > 32 ? (size_t)block * H * sizeof(T) : 0;
-  cudaError_t e = launch_kernel(slell_spmv_kernel<T, E, H, W, VAR, DIAG, LANES>, dim3(grid),
-                                dim3(block), smem, stream, args.pdl != 0, args);
+  cudaError_t e;
+  if constexpr (LANES)
+    e = launch_kernel(slell_spmv_lanes_kernel<T, E, H, W, DIAG>, dim3(grid), dim3(block), smem,
+                      stream, args.pdl != 0, args);
+  else
+    e = launch_kernel(slell_spmv_kernel<T, E, H, W, VAR, DIAG>, dim3(grid), dim3(block), smem,
+                      stream, args.pdl != 0, args);
   if (e == cudaSuccess)
     e = cudaPeekAtLastError();
   if (e != cudaSuccess)
@@ -520,9 +567,10 @@ int launch_spmv_lanes(int x_dtype, const ispm_launch_params &p, const ispm_slell
   if (m.n_slices == 0)
     return ISPM_OK;
   if (!x || !y || !m.slice_ptr || (m.n_elms && (!m.elms)) || (m.n_cols_arr && !m.cols) ||
-      !lanes.tile_lane || !lanes.done)
+      !lanes.tile_lane || !lanes.done || !lanes.vt)
     return fail(ISPM_ERR_INVALID, "NULL pointer");
-  if (lanes.out && (!lanes.v || !lanes.part || !lanes.ticket || !lanes.cta_beg || !lanes.cta_cnt))
+  if (lanes.out && (!lanes.v || !lanes.part || !lanes.ticket || !lanes.cta_beg ||
+                    !lanes.cta_cnt || !lanes.lane_tile0))
     return fail(ISPM_ERR_INVALID, "lane dot without its buffers");
   if (m.var_height || 1024u % spmv_cta_rows(p, m) != 0)
     return fail(ISPM_ERR_INVALID, "a CTA of this launch does not fit one 1024-row tile");

@@ -25,16 +25,25 @@ struct SpmvDot {
   double *out2 = nullptr;
 };
 
-// Batched solves (batch.cu): the matrix is a block-diagonal stack of lanes,
-// each padded to whole 1024-row tiles, and every CTA of the launch lies in
-// one tile.  CTAs of lanes with done[lane] != 0 return at once; with `out`
-// set, out[lane] = sum of y_i v_i over the lane's rows (FP64), finished by
-// the lane's last CTA to arrive: the CTAs of lane L are cta_beg[L] ..
-// cta_beg[L] + cta_cnt[L] - 1 of this launch, part[] holds one partial per
-// CTA and ticket[L] is a zero-initialised counter the launch leaves at zero.
+// Batched solves (batch.cu).  The matrix is a block-diagonal stack of
+// systems, each padded to whole 1024-row tiles; the vectors are a stack of
+// lanes (a system's right-hand sides), also tile-padded.  The launch walks
+// virtual tiles vt[0 .. n_vt): vt[k] = (matrix tile, lane tile), the matrix
+// tile relative to this matrix, the lane tile a global vector tile; every CTA
+// lies in one tile and reads x / writes y at its lane's rows, so all lanes
+// of a system share one copy of its matrix (consecutive virtual tiles of a
+// system's lanes reuse it from L2).  CTAs of lanes with done[lane] != 0
+// return at once; with `out` set, out[lane] = sum of y_i v_i over the lane's
+// rows (FP64), finished by the lane's last CTA to arrive: lane L's partials
+// sit at part[cta_beg[L] .. cta_beg[L] + cta_cnt[L]) in tile order
+// (lane_tile0[L]: the lane's first tile) and ticket[L] is a zero-initialised
+// counter the launch leaves at zero.
 struct SpmvLanes {
   const int *tile_lane = nullptr;  // lane of each tile (global tile index)
-  unsigned tile_base = 0;          // global tile of this launch's row 0
+  unsigned tile_base = 0;          // global tile of the lanes' vector row 0
+  const int2 *vt = nullptr;        // virtual tiles of the launch
+  unsigned n_vt = 0;
+  const int *lane_tile0 = nullptr;
   const int *done = nullptr;
   const void *v = nullptr;
   double *out = nullptr;
@@ -51,7 +60,7 @@ struct SpmvLanes {
 int launch_spmv(int x_dtype, const ispm_launch_params &p, const ispm_slell_view &m,
                 const void *x, void *y, cudaStream_t s, const int *skip = nullptr,
                 const SpmvDot *ep = nullptr, bool pdl = false);
-// Lane-segmented launch (fixed slice height, T == E only).
+// Lane-segmented launch (fixed slice height, T == E only; grid: n_vt tiles).
 int launch_spmv_lanes(int x_dtype, const ispm_launch_params &p, const ispm_slell_view &m,
                       const void *x, void *y, cudaStream_t s, const SpmvLanes &lanes);
 // CTAs a launch of matrix m with params p uses (partials a fused dot needs).
