@@ -331,7 +331,18 @@ typedef struct {
                            preconditioner stays SPD, its values lose 16 mantissa
                            bits; A, the reductions and the reliable updates are
                            unchanged) */
+  int reorder;          /* ISPM_REORDER_AUTO (default): renumber the unknowns in
+                           reverse Cuthill-McKee order when that shrinks the
+                           matrix bandwidth at least 4x (a scattered numbering),
+                           so the SpMV gathers become local; b and x stay in the
+                           caller's order.  ISPM_REORDER_RCM: always;
+                           ISPM_REORDER_NONE: never.  Not with a given factor
+                           pair (it is in the caller's order). */
 } ispm_solver_opts;
+
+#define ISPM_REORDER_NONE 0
+#define ISPM_REORDER_RCM 1
+#define ISPM_REORDER_AUTO 2
 
 #define ISPM_PREC_GIVEN 0
 #define ISPM_PREC_FSAI_GPU 1

@@ -52,6 +52,15 @@ int guess_format(int elm_dtype, int n_rows, int n_cols, const int *row_ptr, cons
 int value_map(const HostSlell &m, int n_rows, const int *row_ptr, const int *cols,
               std::vector<unsigned> &pos);
 
+// Reverse Cuthill-McKee order of a symmetric pattern: perm[new] = old.
+void rcm_order(int n, const int *rp, const int *ci, std::vector<int> &perm);
+// max |j - i| over the entries (of P A P^T when inv, inv[old] = new, is given).
+long long bandwidth(int n, const int *rp, const int *ci, const int *inv);
+// P A P^T as a CSR with sorted columns (perm[new] = old, inv[old] = new).
+void permute_csr(int n, const int *rp, const int *ci, const double *v,
+                 const std::vector<int> &perm, const std::vector<int> &inv,
+                 std::vector<int> &orp, std::vector<int> &oci, std::vector<double> &ov);
+
 // Host CSR result (fastainv output).
 struct HostCsr {
   int n_rows = 0, n_cols = 0, n_nz = 0;

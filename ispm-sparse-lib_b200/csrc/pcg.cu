@@ -475,6 +475,24 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// Reordered solves: out[i] = in[perm[i]] (b into the solver's order) and
+// out[perm[i]] = in[i] (x back), i < n.
+__global__ void permute_in_kernel(double *__restrict__ out, const double *__restrict__ in,
+                                  const int *__restrict__ perm, long long n)
+{
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = in[perm[i]];
+}
+
+__global__ void permute_out_kernel(double *__restrict__ out, const double *__restrict__ in,
+                                   const int *__restrict__ perm, long long n)
+{
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[perm[i]] = in[i];
+}
+
 int grid_for(long long n)
 {
   long long blocks = (n + kThreads - 1) / kThreads;
@@ -567,6 +585,9 @@ struct Solver {
   unsigned fsai_fallbacks = 0; // GPU FSAI rows built as Jacobi rows
   double *x64 = nullptr, *r64 = nullptr, *t64 = nullptr, *b64 = nullptr;
   double *b_stage = nullptr, *x_stage = nullptr;  // device copies for host-vector solves
+  // reordered solves: perm[new] = old, and b / x in the solver's order
+  int *perm = nullptr;
+  double *b_perm = nullptr, *x_perm = nullptr;
   void *vec[11] = {};
   enum { R, U, W, M, NV, P, S, Q, Z, D, TT };
   cudaGraphExec_t graph = nullptr;
@@ -887,7 +908,26 @@ struct Solver {
   {
     ISPM_CUDA_TRY(cudaEventRecord(ev_in, user));
     ISPM_CUDA_TRY(cudaStreamWaitEvent(own, ev_in, 0));
-    int e = solve(b, x, stats, own);
+    int e;
+    if (perm) {
+      // solve P A P^T (P x) = P b in the solver's order, then x = P^T (P x)
+      permute_in_kernel<<<grid_for(n), kThreads, 0, own>>>(b_perm, b, perm, n);
+      e = launched("permute b");
+      if (!e)
+        e = solve(b_perm, x_perm, stats, own);
+      if (!e || e == ISPM_ERR_NOT_CONVERGED || e == ISPM_ERR_BREAKDOWN) {
+        cudaError_t me = cudaMemsetAsync(x, 0, (size_t)n_pad * sizeof(double), own);
+        if (me == cudaSuccess)
+          permute_out_kernel<<<grid_for(n), kThreads, 0, own>>>(x, x_perm, perm, n);
+        const int e2 = me == cudaSuccess ? launched("permute x")
+                                         : fail(ISPM_ERR_CUDA, "memset: %s",
+                                                cudaGetErrorString(me));
+        if (e2)
+          e = e2;
+      }
+    } else {
+      e = solve(b, x, stats, own);
+    }
     cudaError_t ce = cudaEventRecord(ev_out, own);
     if (ce == cudaSuccess)
       ce = cudaStreamWaitEvent(user, ev_out, 0);
@@ -1004,6 +1044,7 @@ void ispm_solver_default_opts(ispm_solver_opts *o)
   o->variant = ISPM_PCG_AUTO;
   o->prec = ISPM_PREC_GIVEN;
   o->factor_bf16 = 0;
+  o->reorder = ISPM_REORDER_AUTO;
 }
 
 int ispm_solver_create(int n, const int *row_ptr, const int *cols, const double *vals,
@@ -1041,6 +1082,36 @@ int ispm_solver_create(int n, const int *row_ptr, const int *cols, const double 
   if (S.opts.prec != ISPM_PREC_GIVEN && S.opts.prec != ISPM_PREC_FSAI_GPU)
     return fail(ISPM_ERR_INVALID, "prec %d", S.opts.prec);
   S.have_prec = S.opts.prec == ISPM_PREC_FSAI_GPU || (g1_rp && g2_rp);
+  if (S.opts.reorder != ISPM_REORDER_NONE && S.opts.reorder != ISPM_REORDER_RCM &&
+      S.opts.reorder != ISPM_REORDER_AUTO)
+    return fail(ISPM_ERR_INVALID, "reorder %d", S.opts.reorder);
+  const bool given_pair = S.opts.prec == ISPM_PREC_GIVEN && g1_rp && g2_rp;
+  if (S.opts.reorder == ISPM_REORDER_RCM && given_pair)
+    return fail(ISPM_ERR_INVALID, "reordering needs prec = ISPM_PREC_FSAI_GPU or none (a given "
+                                  "factor pair is in the caller's order)");
+  std::vector<int> perm, inv, prp, pci;
+  std::vector<double> pv;
+  try {
+    if (S.opts.reorder != ISPM_REORDER_NONE && !given_pair) {
+      rcm_order(n, row_ptr, cols, perm);
+      inv.assign(n, 0);
+      for (int i = 0; i < n; i++)
+        inv[perm[i]] = i;
+      const long long bw0 = bandwidth(n, row_ptr, cols, nullptr);
+      const long long bw1 = bandwidth(n, row_ptr, cols, inv.data());
+      // automatic: reorder only a matrix whose numbering is far from banded
+      if (S.opts.reorder == ISPM_REORDER_RCM || 4 * bw1 <= bw0) {
+        permute_csr(n, row_ptr, cols, vals, perm, inv, prp, pci, pv);
+        row_ptr = prp.data();
+        cols = pci.data();
+        vals = pv.data();
+      } else {
+        perm.clear();
+      }
+    }
+  } catch (const std::bad_alloc &) {
+    return fail(ISPM_ERR_NOMEM, "host allocation while reordering");
+  }
   try {
     if (int e = S.Ain.upload(S.inner, S.inner, n, row_ptr, cols, vals))
       return e;
@@ -1095,6 +1166,15 @@ int ispm_solver_create(int n, const int *row_ptr, const int *cols, const double 
   for (double **pp : d64)
     if (int e = S.mem.get(pp, npad))
       return e;
+  if (!perm.empty()) {
+    if (int e = S.mem.get(&S.perm, (size_t)n))
+      return e;
+    ISPM_CUDA_TRY(cudaMemcpy(S.perm, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    if (int e = S.mem.get(&S.b_perm, npad))
+      return e;
+    if (int e = S.mem.get(&S.x_perm, npad))
+      return e;
+  }
   for (int k = 0; k < 11; k++) {
     int e = S.inner == ISPM_F32 ? S.mem.get((float **)&S.vec[k], npad)
                                 : S.mem.get((double **)&S.vec[k], npad);

@@ -570,7 +570,7 @@ class solver_opts(C.Structure):
                 ("max_refinements", C.c_int), ("check_every", C.c_int),
                 ("use_graph", C.c_int), ("replace_ratio_f32", C.c_double),
                 ("replace_ratio_f64", C.c_double), ("variant", C.c_int), ("prec", C.c_int),
-                ("factor_bf16", C.c_int)]
+                ("factor_bf16", C.c_int), ("reorder", C.c_int)]
 
 
 class solve_stats(C.Structure):
@@ -622,7 +622,7 @@ class PCGSolver:
                  max_iters: int = 100000, max_refinements: int = 500,
                  check_every: int = 16, use_graph: bool = True,
                  replace_ratio: float | None = None, variant: str = "auto",
-                 prec: str = "given", factor_bf16: bool = False):
+                 prec: str = "given", factor_bf16: bool = False, reorder: str = "auto"):
         _declare_solver()
         L = _lib()
         o = solver_opts()
@@ -635,6 +635,7 @@ class PCGSolver:
         o.variant = {"auto": 0, "pipelined": 1, "classic": 2}[variant]
         o.prec = {"given": 0, "fsai_gpu": 1}[prec]
         o.factor_bf16 = int(factor_bf16)
+        o.reorder = {"none": 0, "rcm": 1, "auto": 2}[reorder]
         if A.elms.dtype != np.float64:
             raise TypeError("the solver takes the FP64 matrix")
         self._keep = [A, G1, G2]
