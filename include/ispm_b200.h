@@ -331,7 +331,8 @@ typedef struct {
                            preconditioner stays SPD, its values lose 16 mantissa
                            bits; A, the reductions and the reliable updates are
                            unchanged) */
-  int reorder;          /* ISPM_REORDER_AUTO (default): renumber the unknowns in
+  int reorder;          /* ISPM_REORDER_AUTO (default): unless the bandwidth is
+                           already under n / 16, renumber the unknowns in
                            reverse Cuthill-McKee order when that shrinks the
                            matrix bandwidth at least 4x (a scattered numbering),
                            so the SpMV gathers become local; b and x stay in the

@@ -1092,7 +1092,12 @@ int ispm_solver_create(int n, const int *row_ptr, const int *cols, const double 
   std::vector<int> perm, inv, prp, pci;
   std::vector<double> pv;
   try {
-    if (S.opts.reorder != ISPM_REORDER_NONE && !given_pair) {
+    // automatic mode skips matrices whose band is already under n / 16 (a
+    // mesh in its natural order) without computing an ordering
+    const bool try_rcm = S.opts.reorder == ISPM_REORDER_RCM ||
+                         (S.opts.reorder == ISPM_REORDER_AUTO && !given_pair &&
+                          16 * bandwidth(n, row_ptr, cols, nullptr) >= (long long)n);
+    if (try_rcm) {
       rcm_order(n, row_ptr, cols, perm);
       inv.assign(n, 0);
       for (int i = 0; i < n; i++)
