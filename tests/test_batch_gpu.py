@@ -148,3 +148,20 @@ def test_batch_rejects_bad_args(ispm, cuda, gen):
         ispm.BatchSolver([A], [0])
     with pytest.raises(ispm.IspmError):
         ispm.BatchSolver([A], [1], check_every=0)
+
+
+def test_batch_single_lane_and_tiny_system(ispm, oracle, cuda, gen):
+    """One lane only, and a 1 x 1 system next to a larger one."""
+    A = gen.lognormal_stencil(10, 7, 1.0, 8)
+    b = np.random.default_rng(1).uniform(-1, 1, A.n_rows)
+    B = ispm.BatchSolver([A], 1, inner=np.float32, tol=1e-9)
+    xs, lanes, tot = B.solve_host([b])
+    assert tot["converged"] and B.lanes == 1
+    r = b - oracle.csr_spmv_f64(A.row_ptr, A.cols, A.elms, xs[0])
+    assert np.linalg.norm(r) <= 1e-9 * 1.001 * np.linalg.norm(b)
+    one = ispm.csr_matrix(1, 1, np.array([0, 1], np.int32), np.array([0], np.int32),
+                          np.array([4.0]))
+    B2 = ispm.BatchSolver([one, A], [1, 1], inner=np.float64, tol=1e-9)
+    xs2, lanes2, tot2 = B2.solve_host([np.array([2.0]), b])
+    assert tot2["converged"], lanes2
+    assert abs(xs2[0][0] - 0.5) <= 1e-12
