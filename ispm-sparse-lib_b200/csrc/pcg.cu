@@ -1039,7 +1039,7 @@ void ispm_solver_default_opts(ispm_solver_opts *o)
   o->max_refinements = 500;
   o->check_every = 16;
   o->use_graph = 1;
-  o->replace_ratio_f32 = 1e-1;
+  o->replace_ratio_f32 = 1e-2;
   o->replace_ratio_f64 = 1e-4;
   o->variant = ISPM_PCG_AUTO;
   o->prec = ISPM_PREC_GIVEN;
