@@ -41,6 +41,7 @@
 #include "cuda_util.cuh"
 #include "fsai.h"
 #include "operator.h"
+#include "pcg_state.h"
 #include "sblas_impl.h"
 #include "spmv_launch.h"
 
@@ -49,25 +50,6 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kMaxBlocks = 1024;
-
-enum Done { kRunning = 0, kConverged = 1, kBreakdown = 2, kCap = 3, kReplace = 4 };
-
-// Device-resident solver scalars.
-struct PcgState {
-  double gamma, gammaold, delta, alpha, beta;
-  double rr;       // ||r||^2 of the recursive residual
-  double rr_ref;   // ||r||^2 at the last reliable update
-  double thresh2;  // recursive residual target (absolute, squared)
-  double ru2;      // replacement trigger: rr < ru2 * rr_ref
-  double res2;     // ||b - A x||^2 of the last true residual
-  double pq;       // classic CG: p.Ap
-  double rz;       // classic CG: r.z of the current direction
-  double rz_new;   // classic CG: r.z of the updated residual
-  int it;          // iterations since the last full restart
-  int max_it;      // iteration cap for this restart
-  int done;        // Done
-  int fresh;       // classic CG: next direction update starts a new sequence
-};
 
 struct Scratch {
   double *part;  // 4 * kMaxBlocks partials
@@ -308,19 +290,6 @@ __global__ void __launch_bounds__(kThreads)
 // ---- classic PCG (one recurrence, r; the dots p.Ap and r.z come fused out
 // of the SpMVs that produce Ap and z) ----------------------------------------
 
-// Set the stop / replacement flags after the residual update.
-__device__ __forceinline__ void cg_flags(PcgState *st, double rr)
-{
-  if (!isfinite(rr))
-    st->done = kBreakdown;
-  else if (rr <= st->thresh2)
-    st->done = kConverged;
-  else if (rr < st->ru2 * st->rr_ref)
-    st->done = kReplace;
-  else if (st->it >= st->max_it)
-    st->done = kCap;
-}
-
 // alpha = rz / pq; d += alpha p; r -= alpha q.
 // Without a preconditioner (noprec) also rr = ||r||^2 (= r.z) and the stop
 // test, finished in the last block.  With one, r.r comes with r.z from the
@@ -398,9 +367,7 @@ __global__ void __launch_bounds__(kThreads)
     return;
   if (!noprec) {
     const double rr = st->rr;
-    const bool stop = !isfinite(rr) || rr <= st->thresh2 || rr < st->ru2 * st->rr_ref ||
-                      st->it >= st->max_it;
-    if (stop) {
+    if (cg_stop(st, rr)) {
       if (blockIdx.x == 0 && threadIdx.x == 0)
         cg_flags(st, rr);
       return;
