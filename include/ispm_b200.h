@@ -361,6 +361,10 @@ typedef struct {
   double seconds;       /* host wall time of the solve call */
 } ispm_solve_stats;
 
+/* Defaults: FP32 inner with FP64 reliable updates, tol 1e-10, max_iters
+ * 100000, max_refinements 500, check_every 16, use_graph 1,
+ * replace_ratio_f32 1e-2, replace_ratio_f64 1e-4, variant AUTO, prec GIVEN,
+ * factor_bf16 0, reorder AUTO. */
 void ispm_solver_default_opts(ispm_solver_opts *opts);
 
 typedef struct ispm_solver ispm_solver;
