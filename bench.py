@@ -783,6 +783,7 @@ def main():
         out = {
             "metric": METRIC, "value": t_best, "unit": "s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_best * 1e3,
+            "ms_per_step_median": float(np.median(ms_best)),
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "grid": args.grid, "rows": A.n_rows,
