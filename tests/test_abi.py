@@ -60,3 +60,18 @@ def test_invalid_arguments_raise(ispm, gen):
         ispm.csr_to_slell(bad, 32, 1, False, True)
     with pytest.raises(ispm.IspmError):
         ispm.fastainv_sym(ispm.csr_matrix(0, 0, [0], [], []))
+
+
+def test_solver_default_options(ispm):
+    """ispm_solver_default_opts fills the values the header documents (no GPU
+    needed: it only writes the struct)."""
+    import ctypes as C
+    L = ispm.lib_handle()
+    L.ispm_solver_default_opts.argtypes = [C.POINTER(ispm.solver_opts)]
+    L.ispm_solver_default_opts.restype = None
+    o = ispm.solver_opts()
+    L.ispm_solver_default_opts(C.byref(o))
+    assert o.inner_dtype == ispm.F32 and o.tol == 1e-10
+    assert (o.max_iters, o.max_refinements, o.check_every, o.use_graph) == (100000, 500, 16, 1)
+    assert o.replace_ratio_f32 == 1e-2 and o.replace_ratio_f64 == 1e-4
+    assert (o.variant, o.prec, o.factor_bf16, o.reorder) == (0, 0, 0, 2)
