@@ -63,9 +63,14 @@ def parse():
     p.add_argument("--tol", type=float, default=1e-10)
     p.add_argument("--cpu-sample-iters", type=int, default=20)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--kernel-only", choices=["spmv32", "spmv64"], default=None,
-                   help="only launch the A SpMV of the workload (FP32 or FP64) --reps times "
+    p.add_argument("--kernel-only", choices=["spmv32", "spmv64", "spmv16"], default=None,
+                   help="only launch the A SpMV of the workload (FP32, FP64, or the FP16 "
+                        "split the matrix_f16 solver option stores) --reps times "
                         "(a small program for ncu captures)")
+    p.add_argument("--matrix", choices=["f32", "f16"], default="f32",
+                   help="how the headline mixed solve stores A for its inner iterations: "
+                        "FP32, or FP16 off-diagonals + corrected FP32 diagonal (matrix_f16); "
+                        "the other one is timed beside it")
     p.add_argument("--reps", type=int, default=5)
     p.add_argument("--workload", choices=["c2", "c3", "c4"], default="c2",
                    help="c2: the 128^3 27-point system (default); c3: the 192^3 "
@@ -81,6 +86,16 @@ def kernel_only(args):
     import ispm.gen as gen
     ispm.ispm_initialize()
     A = gen.stencil_grf(args.grid, 27, 8.0, 1.5, 0)
+    if args.kernel_only == "spmv16":
+        d = ispm.device_split_f16(A)
+        p = ispm.default_launch_params(d, np.float32)
+        x = torch.rand(A.n_cols, dtype=torch.float32, device="cuda")
+        y = torch.zeros(d.view().n_rows, dtype=torch.float32, device="cuda")
+        for _ in range(args.reps):
+            d.apply(p, x, y)
+        torch.cuda.synchronize()
+        log(f"[kernel-only] spmv16 {p} x{args.reps} done")
+        return
     dt = np.float32 if args.kernel_only == "spmv32" else np.float64
     Ae = ispm.csr_matrix(A.n_rows, A.n_cols, A.row_ptr, A.cols, A.elms.astype(dt))
     B = ispm.csr_to_slell_guess_format(Ae)
@@ -167,11 +182,12 @@ def oracle_spmv(A, x):
     return A.to_scipy() @ x
 
 
-def algorithmic_bytes(view, vec_bytes):
-    """4|slice_ptr| + 4 (explicit column indices) + sizeof(E) nnz + sizeof(T)(n_cols + n_rows)."""
-    esz = 4 if view.elm_dtype == 0 else 8
+def algorithmic_bytes(view, vec_bytes, split_rows=0):
+    """4|slice_ptr| + 4 (explicit column indices) + sizeof(E) nnz + sizeof(T)(n_cols + n_rows),
+    plus 4 bytes per row of a split operator's FP32 diagonal."""
+    esz = {0: 4, 1: 8, 2: 2, 3: 2}[view.elm_dtype]
     return (4 * view.n_slice_ptr + 4 * view.n_cols_arr + esz * view.n_nz +
-            vec_bytes * (view.n_cols + view.n_rows))
+            vec_bytes * (view.n_cols + view.n_rows) + 4 * split_rows)
 
 
 def measured_peak():
@@ -657,9 +673,14 @@ def main():
     # headline pipeline: FSAI factor built on the GPU + mixed-precision PCG
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    best = ispm.PCGSolver(A, None, None, inner=np.float32, tol=args.tol, prec="fsai_gpu")
+    f16 = args.matrix == "f16"
+    best = ispm.PCGSolver(A, None, None, inner=np.float32, tol=args.tol, prec="fsai_gpu",
+                          matrix_f16=f16)
     torch.cuda.synchronize()
     t_setup = time.perf_counter() - t0
+    # the same pipeline with A's inner copy stored the other way
+    alt = ispm.PCGSolver(A, None, None, inner=np.float32, tol=args.tol, prec="fsai_gpu",
+                         matrix_f16=not f16)
     # the same mixed PCG on the host-built AINV pair, and the plain FP64
     # pipelined PCG on that pair (the reference's method run on this GPU)
     t0 = time.time()
@@ -717,13 +738,15 @@ def main():
     relres = float(np.linalg.norm(b - oracle_spmv(A, x_host)) / np.linalg.norm(b))
     k_side = max(1, min(args.steps, 3))
     for _ in range(max(1, min(args.warmup, 2))):
+        alt.solve(bd, xd, stream)
         mixed.solve(bd, xd, stream)
         plain.solve(bd, xd, stream)
         learned.solve(bd, xd, stream)
+    ms_alt, st_alt = timed(alt, k_side, "mixed+GPU FSAI, other matrix storage")
     ms_mixed, st_mixed = timed(mixed, k_side, "mixed+AINV")
     ms_plain, st_plain = timed(plain, k_side, "plain FP64+AINV")
     ms_learned, st_learned = timed(learned, k_side, "mixed+learned AINV")
-    del mixed, learned
+    del mixed, learned, alt
 
     # end to end through the public API: host b in, host x out, every step
     pin_b = torch.from_numpy(b.copy()).pin_memory()
@@ -736,36 +759,53 @@ def main():
     e2e = (time.perf_counter() - t0) / args.steps
     relres_e2e = float(np.linalg.norm(b - oracle_spmv(A, pin_x.numpy())) / np.linalg.norm(b))
 
-    # dominant kernel: the FP32 SpMV of A inside the mixed solve
+    # dominant kernel: the SpMV of A inside the mixed solve, FP32-stored and
+    # FP16-split, each timed alone (the headline's storage is the roofline line)
     A32 = ispm.csr_matrix(A.n_rows, A.n_cols, A.row_ptr, A.cols, A.elms.astype(np.float32))
     B32 = ispm.csr_to_slell_guess_format(A32)
     d32 = B32.upload()
-    p = ispm.default_launch_params(d32, np.float32)
+    d16 = ispm.device_split_f16(A)
     xs = torch.rand(A.n_cols, dtype=torch.float32, device="cuda")
     ys = torch.zeros(B32.n_rows, dtype=torch.float32, device="cuda")
     reps = 50
-    for _ in range(5):
-        ispm.launch_spmv_kernel(p, d32, xs, ys, stream)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(reps):
-        ispm.launch_spmv_kernel(p, d32, xs, ys, stream)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    t_spmv = e0.elapsed_time(e1) / reps * 1e-3
-    alg = algorithmic_bytes(B32.view(), 4)
+
+    def time_spmv(launch):
+        for _ in range(5):
+            launch()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            launch()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps * 1e-3
+
+    p32 = ispm.default_launch_params(d32, np.float32)
+    p16 = ispm.default_launch_params(d16, np.float32)
+    t32 = time_spmv(lambda: ispm.launch_spmv_kernel(p32, d32, xs, ys, stream))
+    ys16 = torch.zeros(d16.view().n_rows, dtype=torch.float32, device="cuda")
+    t16 = time_spmv(lambda: d16.apply(p16, xs, ys16, stream))
+    alg32 = algorithmic_bytes(B32.view(), 4)
+    alg16 = algorithmic_bytes(d16.view(), 4, split_rows=d16.view().n_rows)
     peak, peak_src = measured_peak()
+    if f16:
+        t_spmv, alg, p = t16, alg16, p16
+        kname = "slell_spmv_kernel<float,__half,H,1,V0,D1> (A split: FP16 off-diagonals)"
+    else:
+        t_spmv, alg, p = t32, alg32, p32
+        kname = "slell_spmv_kernel<float,float,H,1,V0,D1> (A, FP32)"
     achieved = alg / t_spmv / 1e9
 
     t_best = float(np.mean(ms_best)) * 1e-3
     t_mixed = float(np.mean(ms_mixed)) * 1e-3
     t_plain = float(np.mean(ms_plain)) * 1e-3
     t_learned = float(np.mean(ms_learned)) * 1e-3
+    t_alt = float(np.mean(ms_alt)) * 1e-3
     if world > 1:
-        tt = torch.tensor([t_best, e2e, t_mixed, t_plain, t_learned], dtype=torch.float64,
-                          device="cuda")
+        tt = torch.tensor([t_best, e2e, t_mixed, t_plain, t_learned, t_alt],
+                          dtype=torch.float64, device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_best, e2e, t_mixed, t_plain, t_learned = tt.tolist()
+        t_best, e2e, t_mixed, t_plain, t_learned, t_alt = tt.tolist()
     it_l, it_m = st_learned[-1]["iterations"], st_mixed[-1]["iterations"]
 
     # classic FP32 iteration: A SpMV (+p.Ap), r/x update, G SpMV, G^T SpMV
@@ -790,9 +830,17 @@ def main():
                        "nnz": A.n_nz, "tol": args.tol,
                        "method": "mixed FP32/FP64 PCG (classic, FP64 reliable updates), "
                                  "FSAI factor on A's lower pattern built on the GPU",
+                       "inner_matrix": ("FP16 off-diagonals x 2^k + FP32 corrected diagonal"
+                                        if f16 else "FP32"),
                        "parallelism": f"replicas x{world}", "l2": "inputs larger than L2"},
             "iterations": it_best, "reliable_updates": cycles, "true_relres": relres,
             "setup_s": t_setup,
+            "other_inner_matrix": {"inner_matrix": "FP32" if f16 else "FP16 split",
+                                   "solve_s": t_alt, "iterations": st_alt[-1]["iterations"],
+                                   "reliable_updates": st_alt[-1]["refinements"]},
+            "spmv_a_alone": {"fp32_us": t32 * 1e6, "fp32_gbs": alg32 / t32 / 1e9,
+                             "fp32_alg_bytes": alg32, "f16_split_us": t16 * 1e6,
+                             "f16_split_gbs": alg16 / t16 / 1e9, "f16_split_alg_bytes": alg16},
             "mixed_ainv": {"solve_s": t_mixed, "iterations": st_mixed[-1]["iterations"],
                            "nnz_G": G1.n_nz, "droptol": args.droptol,
                            "fastainv_host_s": t_ainv},
@@ -810,7 +858,7 @@ def main():
             "speedup_vs_plain_fp64": t_plain / t_best,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": profile_traffic(),
-                         "kernel": "slell_spmv_kernel<float,float,H,1,V0,D1> (A, FP32)",
+                         "kernel": kname,
                          "launch": f"N={p.N} S={p.S} H={p.H}",
                          "algorithmic_bytes": alg, "us_per_launch": t_spmv * 1e6,
                          "peak_source": peak_src},

@@ -18,6 +18,7 @@
 #define ISPM_B200_H
 
 #include <stddef.h>
+#include <stdint.h>
 
 #ifdef __cplusplus
 extern "C" {
@@ -34,10 +35,11 @@ extern "C" {
 #define ISPM_ERR_TIMEOUT 7        /* a bounded device-side wait ran out */
 #define ISPM_ERR_TOO_LARGE 8      /* size beyond a documented maximum */
 
-/* element / vector types (ISPM_BF16: solver-internal element arrays only) */
+/* element / vector types (ISPM_BF16, ISPM_F16: solver-internal element arrays only) */
 #define ISPM_F32 0
 #define ISPM_F64 1
 #define ISPM_BF16 2
+#define ISPM_F16 3
 
 const char *ispm_error_string(int status);
 /* Message of the calling thread's most recent failing call ("" if none). */
@@ -70,7 +72,7 @@ typedef struct {
   unsigned hblock;     /* 1, 2 or 4 */
   int var_height;
   int diags;
-  int elm_dtype;       /* ISPM_F32 / ISPM_F64 */
+  int elm_dtype;       /* ISPM_F32 / ISPM_F64 (ISPM_F16: ispm_launch_spmv_split) */
   unsigned min_slice_height; /* shortest / tallest slice (equal unless var_height) */
   unsigned max_slice_height;
   long long n_slice_ptr;
@@ -154,6 +156,17 @@ int ispm_launch_params_valid(const ispm_launch_params *p);
  * slice height (fixed-height matrices) and N * H >= every slice's height. */
 int ispm_launch_spmv(int x_dtype, const ispm_launch_params *p, const ispm_slell_view *m,
                      const void *x, void *y, void *stream);
+
+/* Split-operator SpMV (no counterpart in the reference): y = inv_scale *
+ * (A_off x) + diag .* x with FP32 x and y, where m holds the off-diagonal
+ * part as FP16 elements (elm_dtype ISPM_F16, e.g. the split of
+ * ispm_csr_split_f16 converted with ispm_csr_to_slell and its element array
+ * stored as binary16) and diag holds m->n_rows FP32 values (0 on padded
+ * rows), 16-byte aligned.  This is the product the solver's matrix_f16 inner
+ * iterations run; same launch parameters as ispm_launch_spmv. */
+int ispm_launch_spmv_split(const ispm_launch_params *p, const ispm_slell_view *m,
+                           const float *diag, float inv_scale, const float *x, float *y,
+                           void *stream);
 
 /* Launch shape the library picks for a matrix without timing anything (the
  * DEFAULT plan's choice; plan/plan.h:74-96 uses N = 512, H = 1 there). */
@@ -299,6 +312,19 @@ int ispm_fastainv_sym_ex(int out_dtype, int n, const int *row_ptr, const int *co
 int ispm_fsai_sym_gpu(int out_dtype, int n, const int *row_ptr, const int *cols,
                       const double *elms, ispm_csr **ainv1, ispm_csr **ainv2,
                       unsigned *fallbacks);
+/* The FP16 split of a square FP64 CSR matrix that the solver's matrix_f16
+ * option stores (no counterpart in the reference, whose matrices are FP32 or
+ * FP64).  For every row i: off-diagonal values a_ij become
+ * h_ij = fp16(a_ij * scale) (round to nearest even, subnormals kept), written
+ * as IEEE binary16 bit patterns to off_f16[k] for CSR entry k (0 for the
+ * diagonal entry); diag[i] = fp32(a_ii + sum_j (|h_ij| / scale - |a_ij|)),
+ * the diagonal moved by the rounding of the row's off-diagonal magnitudes so
+ * that the split matrix minus A is the weighted graph Laplacian of the
+ * rounding errors (zero row sums for an M-matrix).  scale is the power of
+ * two that maps the largest off-diagonal magnitude into [2^13, 2^14).
+ * off_f16 has row_ptr[n] entries, diag n. */
+int ispm_csr_split_f16(int n, const int *row_ptr, const int *cols, const double *vals,
+                       uint16_t *off_f16, float *diag, float *scale);
 int ispm_csr_get_info(const ispm_csr *m, int *n_rows, int *n_cols, int *n_nz, int *dtype);
 /* Host views of the CSR arrays; valid until ispm_csr_free. */
 int ispm_csr_get_arrays(const ispm_csr *m, const int **row_ptr, const int **cols,
@@ -339,6 +365,18 @@ typedef struct {
                            caller's order.  ISPM_REORDER_RCM: always;
                            ISPM_REORDER_NONE: never.  Not with a given factor
                            pair (it is in the caller's order). */
+  int matrix_f16;       /* FP32 inner solve: store A for the inner iterations as
+                           FP16 off-diagonal values (times a power-of-two scale)
+                           plus an FP32 diagonal, the split of
+                           ispm_csr_split_f16.  The inner matrix then differs
+                           from A by a weighted graph Laplacian of at most 2^-11
+                           times A's own off-diagonal weights, so it keeps A's
+                           near-null space (row sums) and the FP64 reliable
+                           updates still converge; each inner SpMV reads about
+                           half the matrix bytes.  replace_ratio_f32 is raised
+                           to at least 3e-2 (a reliable update at least every
+                           33x fall of the recursive residual).  A and its
+                           reliable-update residuals stay FP64. */
 } ispm_solver_opts;
 
 #define ISPM_REORDER_NONE 0

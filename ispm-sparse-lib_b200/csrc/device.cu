@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "cuda_util.cuh"
+#include "operator.h"
 #include "spmv_launch.h"
 
 namespace ispm {
@@ -94,6 +95,46 @@ int DeviceSlell::upload(const HostSlell &h, bool bf16_values)
     ISPM_CUDA_TRY(
         cudaMemcpy(elms, h.elms_ptr(), ne * elm_size(h.elm_dtype), cudaMemcpyHostToDevice));
   }
+  return ISPM_OK;
+}
+
+int DeviceSlell::upload_f16(const HostSlell &h)
+{
+  if (h.elm_dtype != ISPM_F32)
+    return fail(ISPM_ERR_INVALID, "FP16 storage converts an FP32 element array");
+  // the structure arrays travel unchanged, the elements as binary16
+  std::vector<uint16_t> b(h.n_elms());
+  for (size_t k = 0; k < b.size(); k++) {
+    const double v = h.elms_f[k];
+    b[k] = f16_bits(v);
+    if (f16_value(b[k]) != v)
+      return fail(ISPM_ERR_INVALID, "element %zu (%g) is not a binary16 value", k, v);
+  }
+  release();
+  meta = h.view();
+  meta.elm_dtype = ISPM_F16;
+  const size_t nsp = h.slice_ptr.size(), nc = h.cols.size(), ne = b.size();
+  auto alloc = [](void **p, size_t bytes) -> int {
+    cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+    if (e != cudaSuccess) {
+      *p = nullptr;
+      cudaGetLastError();
+      return fail(e == cudaErrorMemoryAllocation ? ISPM_ERR_NOMEM : ISPM_ERR_CUDA,
+                  "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    }
+    return ISPM_OK;
+  };
+  int st;
+  if ((st = alloc((void **)&slice_ptr, nsp * 4)) || (st = alloc((void **)&cols, nc * 4)) ||
+      (st = alloc(&elms, ne * 2))) {
+    release();
+    return st;
+  }
+  ISPM_CUDA_TRY(cudaMemcpy(slice_ptr, h.slice_ptr.data(), nsp * 4, cudaMemcpyHostToDevice));
+  if (nc)
+    ISPM_CUDA_TRY(cudaMemcpy(cols, h.cols.data(), nc * 4, cudaMemcpyHostToDevice));
+  if (ne)
+    ISPM_CUDA_TRY(cudaMemcpy(elms, b.data(), ne * 2, cudaMemcpyHostToDevice));
   return ISPM_OK;
 }
 

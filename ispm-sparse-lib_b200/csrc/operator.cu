@@ -1,6 +1,8 @@
 // Solver operators (operator.h).
 #include "operator.h"
 
+#include <cmath>
+#include <cstring>
 #include <utility>
 
 #include "cuda_util.cuh"
@@ -108,11 +110,157 @@ int Operator::upload(int vec_dtype, int elm_dtype, int n, const int *rp, const i
   return ISPM_OK;
 }
 
+uint16_t f16_bits(double v)
+{
+  const uint16_t sign = std::signbit(v) ? 0x8000u : 0u;
+  const double a = std::fabs(v);
+  if (a == 0.0)
+    return sign;
+  // quantum of the binade of a (2^-24 below the normal range), then round to
+  // a multiple of it, ties to even (nearbyint under the default rounding mode)
+  int e;
+  std::frexp(a, &e);  // a = f * 2^e, f in [0.5, 1)
+  const int qe = std::max(e - 11, -24);
+  const double r = std::ldexp(std::nearbyint(std::ldexp(a, -qe)), qe);
+  if (r < 0x1p-14)  // subnormal
+    return (uint16_t)(sign | (uint16_t)std::ldexp(r, 24));
+  int er;
+  const double fr = std::frexp(r, &er);  // r = fr * 2^er, fr in [0.5, 1)
+  const unsigned exp_field = (unsigned)(er - 1 + 15);
+  const unsigned mant = (unsigned)std::ldexp(fr * 2.0 - 1.0, 10);
+  return (uint16_t)(sign | (exp_field << 10) | mant);
+}
+
+double f16_value(uint16_t h)
+{
+  const double s = (h & 0x8000u) ? -1.0 : 1.0;
+  const unsigned ef = (h >> 10) & 0x1fu, m = h & 0x3ffu;
+  if (ef == 0)
+    return s * std::ldexp((double)m, -24);
+  return s * std::ldexp(1.0 + (double)m / 1024.0, (int)ef - 15);
+}
+
+int split_f16(int n, const int *rp, const int *ci, const double *v, uint16_t *off, float *diag,
+              float &scale)
+{
+  double amax = 0.0;
+  const long long nnz = rp[n];
+  for (long long k = 0; k < nnz; k++)
+    if (!std::isfinite(v[k]))
+      return fail(ISPM_ERR_INVALID, "FP16 split: non-finite value at entry %lld", k);
+  for (int i = 0; i < n; i++)
+    for (int k = rp[i]; k < rp[i + 1]; k++)
+      if (ci[k] != i)
+        amax = std::max(amax, std::fabs(v[k]));
+  // the largest magnitude lands in [2^13, 2^14): room below the binary16
+  // maximum (65504), 27 binades above its normal range
+  int e = 0;
+  if (amax > 0.0)
+    std::frexp(amax, &e);  // amax in [2^(e-1), 2^e)
+  const int se = amax > 0.0 ? 14 - e : 0;
+  if (se > 127 || se < -126)
+    return fail(ISPM_ERR_INVALID, "FP16 split: off-diagonal magnitudes out of FP32 scale range");
+  const double sc = std::ldexp(1.0, se);
+  for (int i = 0; i < n; i++) {
+    double d = 0.0, corr = 0.0;
+    for (int k = rp[i]; k < rp[i + 1]; k++) {
+      if (ci[k] == i) {
+        d += v[k];
+        off[k] = 0;
+        continue;
+      }
+      const uint16_t h = f16_bits(v[k] * sc);
+      off[k] = h;
+      corr += std::fabs(f16_value(h)) / sc - std::fabs(v[k]);
+    }
+    diag[i] = (float)(d + corr);
+  }
+  scale = (float)sc;
+  return ISPM_OK;
+}
+
+int Operator::upload_split_f16(int n, const int *rp, const int *ci, const double *v)
+{
+  const long long nnz = rp[n];
+  std::vector<uint16_t> h16((size_t)nnz);
+  std::vector<float> dg((size_t)n);
+  float sc = 1.f;
+  if (int st = split_f16(n, rp, ci, v, h16.data(), dg.data(), sc))
+    return st;
+  // off-diagonal CSR with the scaled binary16 values (exact in FP32)
+  std::vector<int> orp((size_t)n + 1), oci;
+  std::vector<double> ov;
+  oci.reserve((size_t)nnz);
+  ov.reserve((size_t)nnz);
+  orp[0] = 0;
+  for (int i = 0; i < n; i++) {
+    for (int k = rp[i]; k < rp[i + 1]; k++)
+      if (ci[k] != i) {
+        oci.push_back(ci[k]);
+        ov.push_back(f16_value(h16[(size_t)k]));
+      }
+    orp[(size_t)i + 1] = (int)oci.size();
+  }
+  std::vector<float> vf;
+  const void *vals = typed_values(ISPM_F32, ov.data(), ov.size(), vf);
+  std::vector<ispm_slell_params> cands;
+  candidate_shapes(ISPM_F32, n, n, orp.data(), oci.data(), vals, false, cands);
+  HostSlell best;
+  size_t best_bytes = ~(size_t)0;
+  for (const ispm_slell_params &c : cands) {
+    HostSlell h;
+    if (convert_csr(ISPM_F32, n, n, orp.data(), oci.data(), vals, (int)c.S, (int)c.H, c.V != 0,
+                    c.D != 0, 4, h))
+      continue;
+    const size_t bytes = stored_bytes(h);
+    if (bytes < best_bytes) {
+      best_bytes = bytes;
+      best = std::move(h);
+      fmt = c;
+    }
+  }
+  if (best_bytes == ~(size_t)0)
+    return fail(ISPM_ERR_INVALID, "no sliced-ELL shape accepted the off-diagonal part");
+  clear_error();
+  if (int st = dev.upload_f16(best))
+    return st;
+  // the diagonal, zero-padded to the matrix's padded row count
+  const size_t rows = (size_t)dev.meta.n_rows;
+  dg.resize(std::max(rows, (size_t)n), 0.f);
+  float *d = nullptr;
+  cudaError_t e = cudaMalloc(&d, rows * sizeof(float));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(e == cudaErrorMemoryAllocation ? ISPM_ERR_NOMEM : ISPM_ERR_CUDA,
+                "cudaMalloc(%zu): %s", rows * sizeof(float), cudaGetErrorString(e));
+  }
+  diag_mem.reset(d, [](float *q) { cudaFree(q); });
+  diag = d;
+  ISPM_CUDA_TRY(cudaMemcpy(d, dg.data(), rows * sizeof(float), cudaMemcpyHostToDevice));
+  inv_scale = 1.f / sc;
+  lp = default_launch(ISPM_F32, dev.view());
+  return ISPM_OK;
+}
+
 size_t Operator::bytes() const
 {
   const ispm_slell_view m = dev.view();
   const size_t esz = m.elm_dtype == ISPM_F64 ? 8 : m.elm_dtype == ISPM_F32 ? 4 : 2;
-  return 4 * (size_t)m.n_slice_ptr + 4 * (size_t)m.n_cols_arr + esz * (size_t)m.n_elms;
+  return 4 * (size_t)m.n_slice_ptr + 4 * (size_t)m.n_cols_arr + esz * (size_t)m.n_elms +
+         (diag ? 4 * (size_t)m.n_rows : 0);
 }
 
 }  // namespace ispm
+
+extern "C" int ispm_csr_split_f16(int n, const int *row_ptr, const int *cols, const double *vals,
+                                  uint16_t *off_f16, float *diag, float *scale)
+{
+  ispm::clear_error();
+  if (n < 0 || !row_ptr || !cols || (row_ptr[n] && !vals) || !off_f16 || !diag || !scale)
+    return ispm::fail(ISPM_ERR_INVALID, "bad arguments");
+  for (int i = 0; i < n; i++)
+    for (int k = row_ptr[i]; k < row_ptr[i + 1]; k++)
+      if (cols[k] < 0 || cols[k] >= n)
+        return ispm::fail(ISPM_ERR_INVALID, "column %d out of range in row %d", cols[k], i);
+  return ispm::split_f16(n, row_ptr, cols, vals, off_f16, diag, *scale);
+}

@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <memory>
 #include <vector>
 
 #include "spmv_launch.h"
@@ -22,10 +23,25 @@ int choose_format(int elm_dtype, int n_rows, int n_cols, const int *rp, const in
                   const double *v, bool fixed_height, ispm_slell_params &out,
                   size_t *out_bytes = nullptr);
 
+// IEEE binary16 of v, rounded to nearest even (subnormals kept); |v| must be
+// below 65520 (the binary16 overflow threshold).
+uint16_t f16_bits(double v);
+// The value of a binary16 bit pattern (finite patterns only).
+double f16_value(uint16_t h);
+// The FP16 split of a square CSR (ispm_csr_split_f16).
+int split_f16(int n, const int *rp, const int *ci, const double *v, uint16_t *off, float *diag,
+              float &scale);
+
 struct Operator {
   DeviceSlell dev;
   ispm_launch_params lp{};
   ispm_slell_params fmt{};
+  // Split operators (upload_split_f16): FP16 off-diagonal elements times
+  // 1 / inv_scale, plus this FP32 diagonal (device, dev.meta.n_rows entries,
+  // owned by diag_mem).
+  std::shared_ptr<float> diag_mem;
+  float *diag = nullptr;
+  float inv_scale = 1.f;
 
   // Convert (n x n CSR, FP64 values stored as elm_dtype) and upload in the
   // min-bytes shape, or in `force`.  value_pos: CSR entry -> element slot,
@@ -35,9 +51,17 @@ struct Operator {
              const double *v, const ispm_slell_params *force = nullptr,
              std::vector<unsigned> *value_pos = nullptr, bool fixed_height = false,
              bool bf16_values = false);
+  // Upload the FP16 split of an n x n FP64 CSR (split_f16): the off-diagonal
+  // entries in the min-bytes sliced-ELL shape with FP16 elements, the
+  // corrected diagonal as an FP32 vector.  FP32 vectors only.
+  int upload_split_f16(int n, const int *rp, const int *ci, const double *v);
   int apply(int vdt, const void *x, void *y, cudaStream_t s, const int *skip,
             const SpmvDot *ep = nullptr, bool pdl = false) const
   {
+    if (diag) {
+      SpmvSplit sp{diag, inv_scale};
+      return launch_spmv(vdt, lp, dev.view(), x, y, s, skip, ep, pdl, &sp);
+    }
     return launch_spmv(vdt, lp, dev.view(), x, y, s, skip, ep, pdl);
   }
   int apply_lanes(int vdt, const void *x, void *y, cudaStream_t s, const SpmvLanes &ln) const

@@ -50,6 +50,9 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kMaxBlocks = 1024;
+// Smallest reliable-update ratio with an FP16-stored inner matrix
+// (ispm_solver_opts.matrix_f16).
+constexpr double kSplitReplaceRatio = 3e-2;
 
 struct Scratch {
   double *part;  // 4 * kMaxBlocks partials
@@ -785,7 +788,11 @@ struct Solver {
     // the recursive residual must get a little below the target so that the
     // true residual (which it tracks to within the drift) meets it
     const double thresh2 = 0.25 * target * target;
-    const double ru = inner == ISPM_F32 ? opts.replace_ratio_f32 : opts.replace_ratio_f64;
+    double ru = inner == ISPM_F32 ? opts.replace_ratio_f32 : opts.replace_ratio_f64;
+    // an FP16-stored inner matrix drifts further from A between reliable
+    // updates: keep them at most a 33x fall apart
+    if (Ain.diag)
+      ru = std::max(ru, kSplitReplaceRatio);
     const double ru2 = ru * ru;
     bool restart = true;
     int since_restart = 0;
@@ -1012,6 +1019,7 @@ void ispm_solver_default_opts(ispm_solver_opts *o)
   o->prec = ISPM_PREC_GIVEN;
   o->factor_bf16 = 0;
   o->reorder = ISPM_REORDER_AUTO;
+  o->matrix_f16 = 0;
 }
 
 int ispm_solver_create(int n, const int *row_ptr, const int *cols, const double *vals,
@@ -1085,8 +1093,12 @@ int ispm_solver_create(int n, const int *row_ptr, const int *cols, const double 
     return fail(ISPM_ERR_NOMEM, "host allocation while reordering");
   }
   try {
-    if (int e = S.Ain.upload(S.inner, S.inner, n, row_ptr, cols, vals))
+    if (S.inner == ISPM_F32 && S.opts.matrix_f16) {
+      if (int e = S.Ain.upload_split_f16(n, row_ptr, cols, vals))
+        return e;
+    } else if (int e = S.Ain.upload(S.inner, S.inner, n, row_ptr, cols, vals)) {
       return e;
+    }
     if (int e = S.A64.upload(ISPM_F64, ISPM_F64, n, row_ptr, cols, vals, &S.Ain.fmt))
       return e;
     if (S.opts.prec == ISPM_PREC_FSAI_GPU) {

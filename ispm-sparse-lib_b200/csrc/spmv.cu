@@ -16,8 +16,12 @@
 //  * the cross-thread reduction is warp shuffles (xor butterfly, uniform
 //    across the warp so slices of different heights may share one) with a
 //    shared-memory step only when a slice spans several warps;
-//  * hblock columns gather W consecutive x values with one vector load.
+//  * hblock columns gather W consecutive x values with one vector load;
+//  * a split operator (FP16 off-diagonal elements and an FP32 diagonal
+//    vector, the solver's matrix_f16 option) scales the stored sum by a power
+//    of two and adds the diagonal term in the store epilogue.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <type_traits>
@@ -45,6 +49,8 @@ template <class T, class E> struct SpmvArgs {
   SpmvDot ep;         // optional fused epilogue: *ep.out = sum_i y_i v_i (FP64)
   SpmvLanes ln;       // lane-segmented launches only
   int pdl;            // launched as a programmatic dependent of the previous kernel
+  const float *dg;    // split operators (E = __half): FP32 diagonal, one per row
+  float inv_scale;    // split operators: 1 / the power-of-two element scale
 };
 
 // Finish a fused dot product: every block publishes its partial, the last
@@ -371,6 +377,15 @@ __device__ __forceinline__ void spmv_body(const SpmvArgs<T, E> &a)
       }
     }
   }
+  if constexpr (std::is_same<E, __half>::value) {
+    // split operator: y = inv_scale * (stored off-diagonal sum) + diag * x
+    if (active && t < R) {
+      const Vec<H, float> dv = ld_stream<H>(a.dg + y0 + t * H);
+#pragma unroll
+      for (int h = 0; h < H; h++)
+        acc[h] = fma(dv.v[h], ld_x_guard(xp, y0 + t * H + h, a.n_cols), acc[h] * a.inv_scale);
+    }
+  }
   if (active && t < R)
     st_vec<H, T>(yp + y0 + t * H, acc);
   if (LANES ? a.ln.out != nullptr : a.ep.out != nullptr) {
@@ -474,10 +489,18 @@ int launch_h(const SpmvArgs<T, E> &args, const ispm_slell_view &m, unsigned tps,
 template <class T, class E>
 int launch_te(const ispm_launch_params &p, const ispm_slell_view &m, const void *x, void *y,
               cudaStream_t s, const int *skip, const SpmvDot *ep, const SpmvLanes *ln = nullptr,
-              bool pdl = false)
+              bool pdl = false, const SpmvSplit *split = nullptr)
 {
   SpmvArgs<T, E> a;
   a.pdl = pdl ? 1 : 0;
+  a.dg = nullptr;
+  a.inv_scale = 1.f;
+  if constexpr (std::is_same<E, __half>::value) {
+    if (!split || !split->diag || !aligned(split->diag, 16))
+      return fail(ISPM_ERR_INVALID, "FP16 elements need the split operator's diagonal vector");
+    a.dg = split->diag;
+    a.inv_scale = split->inv_scale;
+  }
   a.skip = skip;
   a.ep = ep ? *ep : SpmvDot{};
   a.ln = ln ? *ln : SpmvLanes{};
@@ -517,10 +540,14 @@ int check_launch(int x_dtype, const ispm_launch_params &p, const ispm_slell_view
 {
   const int e = m.elm_dtype;
   if (!((x_dtype == ISPM_F32 && e == ISPM_F32) || (x_dtype == ISPM_F64 && e == ISPM_F32) ||
-        (x_dtype == ISPM_F64 && e == ISPM_F64) || (x_dtype == ISPM_F32 && e == ISPM_BF16)))
+        (x_dtype == ISPM_F64 && e == ISPM_F64) || (x_dtype == ISPM_F32 && e == ISPM_BF16) ||
+        (x_dtype == ISPM_F32 && e == ISPM_F16)))
     return fail(ISPM_ERR_INVALID, "(T, E) = (%s, %s) is not an instantiated pair",
                 x_dtype == ISPM_F64 ? "double" : "float",
-                e == ISPM_F64 ? "double" : e == ISPM_F32 ? "float" : "bfloat16");
+                e == ISPM_F64   ? "double"
+                : e == ISPM_F32 ? "float"
+                : e == ISPM_F16 ? "half"
+                                : "bfloat16");
   if (!is_pow2(p.N) || p.N < 4 || p.N > 1024)
     return fail(ISPM_ERR_INVALID, "N = %u (power of two in [4, 1024])", p.N);
   if (p.H != 1 && p.H != 2 && p.H != 4)
@@ -590,8 +617,10 @@ unsigned spmv_grid(const ispm_launch_params &p, const ispm_slell_view &m)
 
 int launch_spmv(int x_dtype, const ispm_launch_params &p, const ispm_slell_view &m,
                 const void *x, void *y, cudaStream_t s, const int *skip, const SpmvDot *ep,
-                bool pdl)
+                bool pdl, const SpmvSplit *split)
 {
+  if (split && m.elm_dtype != ISPM_F16)
+    return fail(ISPM_ERR_INVALID, "a split diagonal goes with FP16 elements");
   int st = check_launch(x_dtype, p, m);
   if (st)
     return st;
@@ -607,6 +636,8 @@ int launch_spmv(int x_dtype, const ispm_launch_params &p, const ispm_slell_view 
     return fail(ISPM_ERR_INVALID, "NULL pointer");
   if (x_dtype == ISPM_F32 && m.elm_dtype == ISPM_BF16)
     return launch_te<float, __nv_bfloat16>(p, m, x, y, s, skip, ep, nullptr, pdl);
+  if (x_dtype == ISPM_F32 && m.elm_dtype == ISPM_F16)
+    return launch_te<float, __half>(p, m, x, y, s, skip, ep, nullptr, pdl, split);
   if (x_dtype == ISPM_F32)
     return launch_te<float, float>(p, m, x, y, s, skip, ep, nullptr, pdl);
   if (m.elm_dtype == ISPM_F32)
@@ -630,6 +661,20 @@ int ispm_launch_spmv(int x_dtype, const ispm_launch_params *p, const ispm_slell_
   if (!p || !m)
     return ispm::fail(ISPM_ERR_INVALID, "NULL params or matrix");
   return ispm::launch_spmv(x_dtype, *p, *m, x, y, (cudaStream_t)stream);
+}
+
+int ispm_launch_spmv_split(const ispm_launch_params *p, const ispm_slell_view *m,
+                           const float *diag, float inv_scale, const float *x, float *y,
+                           void *stream)
+{
+  ispm::clear_error();
+  if (!p || !m || !diag)
+    return ispm::fail(ISPM_ERR_INVALID, "NULL params, matrix or diagonal");
+  if (m->elm_dtype != ISPM_F16)
+    return ispm::fail(ISPM_ERR_INVALID, "the split product takes FP16 elements");
+  ispm::SpmvSplit sp{diag, inv_scale};
+  return ispm::launch_spmv(ISPM_F32, *p, *m, x, y, (cudaStream_t)stream, nullptr, nullptr,
+                           false, &sp);
 }
 
 }  // extern "C"

@@ -53,13 +53,23 @@ struct SpmvLanes {
   const int *cta_cnt = nullptr;
 };
 
+// Split operator (FP16 off-diagonal elements, elm_dtype ISPM_F16): the launch
+// computes y_i = inv_scale * (sum of the stored entries of row i times x) +
+// diag[i] * x[i], with diag holding one FP32 value per (padded) row, 0 past
+// n_cols.
+struct SpmvSplit {
+  const float *diag = nullptr;
+  float inv_scale = 1.f;
+};
+
 // Validate and launch y = A x on `s`.  `skip` (device int, may be NULL): the
 // kernel returns at once when it holds a nonzero value.
 // pdl: launch as a programmatic dependent of the stream's previous kernel
 // (that kernel's results are read only after it completed).
 int launch_spmv(int x_dtype, const ispm_launch_params &p, const ispm_slell_view &m,
                 const void *x, void *y, cudaStream_t s, const int *skip = nullptr,
-                const SpmvDot *ep = nullptr, bool pdl = false);
+                const SpmvDot *ep = nullptr, bool pdl = false,
+                const SpmvSplit *split = nullptr);
 // Lane-segmented launch (fixed slice height, T == E only; grid: n_vt tiles).
 int launch_spmv_lanes(int x_dtype, const ispm_launch_params &p, const ispm_slell_view &m,
                       const void *x, void *y, cudaStream_t s, const SpmvLanes &lanes);
@@ -84,6 +94,9 @@ struct DeviceSlell {
   }
   // bf16_values: keep an FP32 element array as BF16 (elm_dtype ISPM_BF16)
   int upload(const HostSlell &h, bool bf16_values = false);
+  // Keep an FP32 element array whose values are all exact binary16 values as
+  // FP16 (elm_dtype ISPM_F16).
+  int upload_f16(const HostSlell &h);
   int update_elms(const HostSlell &h);
   void release();
   ~DeviceSlell() { release(); }

@@ -25,6 +25,7 @@ _PKG = os.path.dirname(_HERE)
 LIB_PATH = os.path.join(_PKG, "libispm_b200.so")
 
 F32, F64 = 0, 1
+BF16, F16 = 2, 3  # solver-internal element types
 OK = 0
 ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_ARCH = 1, 2, 3, 4
 ERR_BREAKDOWN, ERR_NOT_CONVERGED, ERR_TIMEOUT, ERR_TOO_LARGE = 5, 6, 7, 8
@@ -381,6 +382,90 @@ def launch_spmv_kernel(params: spmv_launch_params, m, x, y, stream=None):
                                    _ptr(y), _stream(stream)))
 
 
+def csr_split_f16(A: csr_matrix):
+    """The FP16 split the solver's matrix_f16 option stores: (off, diag,
+    scale) with off[k] the binary16 bit pattern (uint16) of A's CSR entry k
+    times scale (0 on diagonal entries) and diag the FP32 diagonal corrected
+    by the rounding of the row's off-diagonal magnitudes."""
+    L = _lib()
+    vp = C.c_void_p
+    L.ispm_csr_split_f16.argtypes = [C.c_int, vp, vp, vp, vp, vp, C.POINTER(C.c_float)]
+    L.ispm_csr_split_f16.restype = C.c_int
+    n = A.row_ptr.size - 1
+    vals = np.ascontiguousarray(A.elms, np.float64)
+    off = np.zeros(max(int(A.row_ptr[n]), 1), np.uint16)
+    diag = np.zeros(max(n, 1), np.float32)
+    sc = C.c_float()
+    _check(L.ispm_csr_split_f16(n, _ptr(A.row_ptr), _ptr(A.cols), _ptr(vals), _ptr(off),
+                                _ptr(diag), C.byref(sc)))
+    return off[: int(A.row_ptr[n])], diag[:n], float(sc.value)
+
+
+class device_split_f16:
+    """Device copy of the FP16 split of an FP64 CSR A (csr_split_f16): the
+    off-diagonal part as sliced-ELL with binary16 elements (shape `fmt` =
+    (S, hblock, var_height, diags), or the reference's guess), the FP32
+    diagonal (n_rows padded entries) and 1 / scale.  Device arrays are torch
+    tensors; `view` describes them for launch_spmv_split."""
+
+    def __init__(self, A: csr_matrix, fmt=None):
+        import torch
+        off, diag, sc = csr_split_f16(A)
+        n = A.row_ptr.size - 1
+        rows = np.repeat(np.arange(n), np.diff(A.row_ptr))
+        keep = A.cols != rows
+        orp = np.zeros(n + 1, np.int32)
+        orp[1:] = np.cumsum(np.bincount(rows[keep], minlength=n))
+        vals = off.view(np.float16)[keep].astype(np.float32)
+        Ao = csr_matrix(n, n, orp, np.ascontiguousarray(A.cols[keep], np.int32), vals)
+        self.host = csr_to_slell_guess_format(Ao) if fmt is None else csr_to_slell(Ao, *fmt)
+        v = self.host.view()
+        el = self.host.elms.astype(np.float16)
+        if not np.array_equal(el.astype(np.float32), self.host.elms):
+            raise IspmError(ERR_INVALID, "split values are not binary16 values")
+        dev = torch.device("cuda")
+        self._sp = torch.from_numpy(self.host.slice_ptr.view(np.int32).copy()).to(dev)
+        self._cols = torch.from_numpy(self.host.cols.view(np.int32).copy() if v.n_cols_arr
+                                      else np.zeros(4, np.int32)).to(dev)
+        self._elms = torch.from_numpy(el if el.size else np.zeros(8, np.float16)).to(dev)
+        dg = np.zeros(v.n_rows, np.float32)
+        dg[:n] = diag
+        self.diag = torch.from_numpy(dg).to(dev)
+        self.scale = sc
+        self.inv_scale = 1.0 / sc
+        dv = slell_view()
+        for f, _ in slell_view._fields_:
+            setattr(dv, f, getattr(v, f))
+        dv.elm_dtype = F16
+        dv.slice_ptr, dv.cols = self._sp.data_ptr(), self._cols.data_ptr()
+        dv.elms = self._elms.data_ptr()
+        self.view_ = dv
+
+    def view(self) -> slell_view:
+        return self.view_
+
+    def bytes(self) -> int:
+        """Stored bytes: slice_ptr + cols + FP16 elements + FP32 diagonal."""
+        v = self.view_
+        return 4 * v.n_slice_ptr + 4 * v.n_cols_arr + 2 * v.n_elms + 4 * v.n_rows
+
+    def apply(self, params: spmv_launch_params, x, y, stream=None):
+        launch_spmv_split(params, self.view_, self.diag, self.inv_scale, x, y, stream)
+
+
+def launch_spmv_split(params: spmv_launch_params, view: slell_view, diag, inv_scale: float,
+                      x, y, stream=None):
+    """y = inv_scale * (A_off x) + diag * x: `view` describes the off-diagonal
+    part with FP16 elements (elm_dtype F16) in device memory."""
+    L = _lib()
+    vp = C.c_void_p
+    L.ispm_launch_spmv_split.argtypes = [C.POINTER(spmv_launch_params), C.POINTER(slell_view),
+                                         vp, C.c_float, vp, vp, vp]
+    L.ispm_launch_spmv_split.restype = C.c_int
+    _check(L.ispm_launch_spmv_split(C.byref(params), C.byref(view), _ptr(diag),
+                                    float(inv_scale), _ptr(x), _ptr(y), _stream(stream)))
+
+
 # ---------------------------------------------------------------------------
 # plan/plan.h
 # ---------------------------------------------------------------------------
@@ -570,7 +655,7 @@ class solver_opts(C.Structure):
                 ("max_refinements", C.c_int), ("check_every", C.c_int),
                 ("use_graph", C.c_int), ("replace_ratio_f32", C.c_double),
                 ("replace_ratio_f64", C.c_double), ("variant", C.c_int), ("prec", C.c_int),
-                ("factor_bf16", C.c_int), ("reorder", C.c_int)]
+                ("factor_bf16", C.c_int), ("reorder", C.c_int), ("matrix_f16", C.c_int)]
 
 
 class solve_stats(C.Structure):
@@ -615,14 +700,16 @@ class PCGSolver:
     None.  inner: np.float64 (plain FP64) or np.float32 (mixed precision: FP32
     matrices / vectors, FP64 reductions).  Reliable updates recompute the
     true residual with the FP64 matrix whenever the recursive residual has
-    fallen by replace_ratio since the previous one."""
+    fallen by replace_ratio since the previous one.  matrix_f16 (FP32 inner
+    only): the inner iterations use the FP16 split of A (csr_split_f16)."""
 
     def __init__(self, A: csr_matrix, G1: csr_matrix | None = None,
                  G2: csr_matrix | None = None, inner=np.float32, tol: float = 1e-10,
                  max_iters: int = 100000, max_refinements: int = 500,
                  check_every: int = 16, use_graph: bool = True,
                  replace_ratio: float | None = None, variant: str = "auto",
-                 prec: str = "given", factor_bf16: bool = False, reorder: str = "auto"):
+                 prec: str = "given", factor_bf16: bool = False, reorder: str = "auto",
+                 matrix_f16: bool = False):
         _declare_solver()
         L = _lib()
         o = solver_opts()
@@ -636,6 +723,7 @@ class PCGSolver:
         o.prec = {"given": 0, "fsai_gpu": 1}[prec]
         o.factor_bf16 = int(factor_bf16)
         o.reorder = {"none": 0, "rcm": 1, "auto": 2}[reorder]
+        o.matrix_f16 = int(matrix_f16)
         if A.elms.dtype != np.float64:
             raise TypeError("the solver takes the FP64 matrix")
         self._keep = [A, G1, G2]
@@ -696,7 +784,7 @@ def default_launch_params(m, x_dtype=None) -> spmv_launch_params:
     L.ispm_default_launch.argtypes = [C.c_int, C.POINTER(slell_view),
                                       C.POINTER(spmv_launch_params)]
     L.ispm_default_launch.restype = C.c_int
-    v = m.view()
+    v = m.view() if hasattr(m, "view") else m
     if x_dtype is None:
         x_dtype = v.elm_dtype
     elif not isinstance(x_dtype, int):
