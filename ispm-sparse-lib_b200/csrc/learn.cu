@@ -6,7 +6,7 @@
 // (fastainv/droptol-tuning.h:4-103).  Here a per-row network predicts, from
 // local matrix features, the drop tolerance of each row of the factor and a
 // diagonal rescale of that row (applied through fastainv_sym_ex); the
-// caller keeps the plain build as the fallback and the judge.
+// caller keeps the plain build as the fallback and the yardstick.
 //
 // Network: y = W3 relu(W2 relu(W1 x + b1) + b2) + b3 with BF16 weights and
 // inputs and FP32 accumulation.  Layers 1 and 2 (and the weight gradients of

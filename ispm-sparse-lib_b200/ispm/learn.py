@@ -18,7 +18,7 @@ iteration, vectors included) is the target of every row of that system.  The res
 trained toward 1: measured row rescales (the modified-AINV row-sum
 compensation at exponents 0.1 .. 1) raised iteration counts on this family.
 
-Plain fastainv_sym stays the fallback and the judge: `gate` accepts the
+Plain fastainv_sym stays the fallback and the yardstick: `gate` accepts the
 learned factor only if PCG iterations drop (and the solve is not slower).
 
   python -m ispm.learn train  [--systems N] [--out PATH]

@@ -1,6 +1,6 @@
 """Sliced-ELL SpMV on the GPU against the CPU oracle (cuda/spmv/kernel.h).
 
-Tolerances (north star): FP64 results within 1e-14 relative, FP32 within
+Tolerances: FP64 results within 1e-14 relative, FP32 within
 1e-6 relative (norm-wise, against the long-double sum of the same stored
 values); every row also within the worst-case forward-error bound
 gamma_k * sum_j |a_ij x_j| of a k-term sum, whatever the summation order.
