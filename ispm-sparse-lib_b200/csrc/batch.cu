@@ -818,6 +818,10 @@ int Batch::build_group(Group &g, const int *const *rp, const int *const *ci,
     return e;
   if ((long long)g.Ain.dev.meta.n_rows != rows || (long long)g.A64.dev.meta.n_rows != rows)
     return fail(ISPM_ERR_INVALID, "stacked operator padded beyond its tiles");
+  // lane-segmented launches walk x through registers (the staged shape is
+  // for single systems)
+  g.Ain.lp = register_walk_launch(inner, g.Ain.dev.view());
+  g.A64.lp = register_walk_launch(ISPM_F64, g.A64.dev.view());
   if (!have_prec)
     return ISPM_OK;
   std::vector<int> g_rp, g_ci, t_rp, t_ci;
@@ -833,6 +837,8 @@ int Batch::build_group(Group &g, const int *const *rp, const int *const *ci,
   if (int e = g.Ht.upload(inner, inner, n, t_rp.data(), t_ci.data(), zeros.data(), &g.h_fmt,
                           &pos_t))
     return e;
+  g.G.lp = register_walk_launch(inner, g.G.dev.view());
+  g.Ht.lp = register_walk_launch(inner, g.Ht.dev.view());
   Mem tmp;
   int *a_rp_d, *a_ci_d, *g_rp_d;
   double *a_v_d, *g_v_d, *gt_v_d;

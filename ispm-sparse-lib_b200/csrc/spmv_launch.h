@@ -104,6 +104,10 @@ struct DeviceSlell {
 
 // B200 launch heuristic for a matrix: threads per slice and rows per thread.
 ispm_launch_params default_launch(int x_dtype, const ispm_slell_view &m);
+// The same heuristic restricted to the register walk (several rows per
+// thread, x gathered through the read-only path): the shapes the
+// lane-segmented launches take.
+ispm_launch_params register_walk_launch(int x_dtype, const ispm_slell_view &m);
 
 // d.elms[map[k]] = vals[k] for k < n (device arrays; vals FP32 or FP64).
 // Same from the slot side: d.elms[s] = vals[inv[s]] for every element slot

@@ -463,3 +463,106 @@ int orc_pcg_f64(int pipelined, int n, const int *A_rp, const int *A_ci, const do
   free(r); free(u); free(w); free(p); free(q); free(s); free(z); free(m); free(nv); free(tmp);
   return it;
 }
+
+/* FSAI rows on A's lower pattern (the construction fsai.cu runs on the GPU):
+ * row i solves A[P,P] y = e_last with P = {j <= i : a_ij != 0} (A's sorted
+ * row i up to its diagonal), then g = y / sqrt(y_last).  Dense Cholesky per
+ * row in FP64; a local matrix that is not positive definite gives the Jacobi
+ * row (1/sqrt(a_ii) when a_ii > 0, else 1). */
+long long orc_fsai_pattern_size(const int *rp, const int *ci, const int *rows, int n_rows_out)
+{
+  long long s = 0;
+  for (int k = 0; k < n_rows_out; k++) {
+    const int i = rows[k];
+    for (int e = rp[i]; e < rp[i + 1] && ci[e] <= i; e++)
+      s++;
+  }
+  return s;
+}
+
+static double csr_at(const int *rp, const int *ci, const double *v, int r, int c)
+{
+  int lo = rp[r], hi = rp[r + 1];
+  while (lo < hi) {
+    int mid = (lo + hi) / 2;
+    if (ci[mid] < c)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return (lo < rp[r + 1] && ci[lo] == c) ? v[lo] : 0.0;
+}
+
+long long orc_fsai_rows(const int *rp, const int *ci, const double *v, const int *rows,
+                        int n_rows_out, int *out_rp, int *out_ci, double *out_v)
+{
+  out_rp[0] = 0;
+  for (int k = 0; k < n_rows_out; k++) {
+    const int i = rows[k];
+    int K = 0;
+    for (int e = rp[i]; e < rp[i + 1] && ci[e] <= i; e++)
+      K++;
+    out_rp[k + 1] = out_rp[k] + K;
+  }
+  long long jacobi = 0;
+  int bad = 0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : jacobi, bad)
+  for (int k = 0; k < n_rows_out; k++) {
+    const int i = rows[k];
+    const int o = out_rp[k], K = out_rp[k + 1] - o;
+    if (K > 64 || K == 0) {
+      bad++;
+      continue;
+    }
+    double L[64][64], y[64];
+    int P[64];
+    for (int a = 0; a < K; a++)
+      P[a] = ci[rp[i] + a];
+    for (int a = 0; a < K; a++)
+      for (int b = 0; b <= a; b++)
+        L[a][b] = csr_at(rp, ci, v, P[a], P[b]);
+    int ok = 1;
+    for (int c = 0; c < K && ok; c++) {
+      double d = L[c][c];
+      for (int t = 0; t < c; t++)
+        d -= L[c][t] * L[c][t];
+      if (!(d > 0.0)) {
+        ok = 0;
+        break;
+      }
+      L[c][c] = sqrt(d);
+      for (int r = c + 1; r < K; r++) {
+        double s = L[r][c];
+        for (int t = 0; t < c; t++)
+          s -= L[r][t] * L[c][t];
+        L[r][c] = s / L[c][c];
+      }
+    }
+    if (!ok) {
+      const double aii = csr_at(rp, ci, v, i, i);
+      for (int a = 0; a < K; a++) {
+        out_ci[o + a] = P[a];
+        out_v[o + a] = 0.0;
+      }
+      out_v[o + K - 1] = aii > 0.0 ? 1.0 / sqrt(aii) : 1.0;
+      jacobi++;
+      continue;
+    }
+    /* L L^T y = e_last: y_last = 1 / L_last^2, then back-substitute with L^T */
+    for (int a = 0; a < K; a++)
+      y[a] = 0.0;
+    y[K - 1] = 1.0 / (L[K - 1][K - 1] * L[K - 1][K - 1]);
+    for (int r = K - 2; r >= 0; r--) {
+      double s = 0.0;
+      for (int c = r + 1; c < K; c++)
+        s += L[c][r] * y[c];
+      y[r] = -s / L[r][r];
+    }
+    const double sc = 1.0 / sqrt(y[K - 1]);
+    for (int a = 0; a < K; a++) {
+      out_ci[o + a] = P[a];
+      out_v[o + a] = y[a] * sc;
+    }
+  }
+  return bad ? -1 : jacobi;
+}

@@ -89,6 +89,18 @@ int orc_pcg_f64(int pipelined, int n, const int *A_rp, const int *A_ci, const do
 /* Number of OpenMP threads the oracle's parallel loops use. */
 int orc_num_threads(void);
 
+/* FSAI factor rows on A's lower pattern, the construction of the GPU build
+ * (ispm-sparse-lib_b200/csrc/fsai.cu): for each listed row i, P = the sorted
+ * entries of row i of A up to the diagonal, A[P,P] y = e_last (dense FP64
+ * Cholesky), g = y / sqrt(y_last); a local matrix that is not positive
+ * definite gives the Jacobi row.  orc_fsai_pattern_size: entries the listed
+ * rows hold.  orc_fsai_rows fills out_rp[n_rows_out + 1], out_ci, out_v and
+ * returns the Jacobi-row count (-1 if a pattern is empty or exceeds 64
+ * entries). */
+long long orc_fsai_pattern_size(const int *rp, const int *ci, const int *rows, int n_rows_out);
+long long orc_fsai_rows(const int *rp, const int *ci, const double *v, const int *rows,
+                        int n_rows_out, int *out_rp, int *out_ci, double *out_v);
+
 #ifdef __cplusplus
 }
 #endif

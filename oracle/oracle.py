@@ -78,6 +78,10 @@ def orc():
         L.orc_pcg_f64.argtypes = [i, i] + [vp] * 9 + [vp, vp, d, i, vp]
         L.orc_pcg_f64.restype = i
         L.orc_num_threads.restype = i
+        L.orc_fsai_pattern_size.argtypes = [vp, vp, vp, i]
+        L.orc_fsai_pattern_size.restype = C.c_longlong
+        L.orc_fsai_rows.argtypes = [vp, vp, vp, vp, i, vp, vp, vp]
+        L.orc_fsai_rows.restype = C.c_longlong
         _orc = L
     return _orc
 
@@ -295,6 +299,27 @@ def fsai_lower_f64(row_ptr, cols, elms):
         g_v.extend(g)
         g_rp.append(len(g_ci))
     return (np.array(g_rp, np.int32), np.array(g_ci, np.int32), np.array(g_v))
+
+
+def fsai_rows_f64(row_ptr, cols, elms, rows):
+    """FSAI rows (same construction as fsai_lower_f64) for the listed rows only,
+    in C with OpenMP: for full-size matrices, or seeded samples of their rows.
+    Returns (row_ptr, cols, vals, jacobi_rows) with row k of the result being
+    row rows[k] of G."""
+    rp = np.ascontiguousarray(row_ptr, np.int32)
+    ci = np.ascontiguousarray(cols, np.int32)
+    v = np.ascontiguousarray(elms, np.float64)
+    rw = np.ascontiguousarray(rows, np.int32)
+    L = orc()
+    nnz = L.orc_fsai_pattern_size(rp.ctypes.data, ci.ctypes.data, rw.ctypes.data, len(rw))
+    orp = np.zeros(len(rw) + 1, np.int32)
+    oci = np.zeros(max(nnz, 1), np.int32)
+    ov = np.zeros(max(nnz, 1), np.float64)
+    jac = L.orc_fsai_rows(rp.ctypes.data, ci.ctypes.data, v.ctypes.data, rw.ctypes.data,
+                          len(rw), orp.ctypes.data, oci.ctypes.data, ov.ctypes.data)
+    if jac < 0:
+        raise ValueError("an FSAI row pattern is empty or exceeds 64 entries")
+    return orp, oci[:nnz], ov[:nnz], int(jac)
 
 
 def pcg_f64(A, b, G1=None, G2=None, pipelined=False, tol=1e-10, max_it=100000, x0=None):
