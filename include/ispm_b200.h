@@ -245,9 +245,9 @@ int ispm_sblas_dot(int dtype, const void *x, const void *y, void *s, int n, void
  * pre-reserved device memory budget, or loops that must not risk the implicit
  * synchronisation of cudaMalloc / cudaFree).  Same arguments and result as
  * ispm_sblas_dot; its scratch is a static device array inside the library
- * (1024 partial sums + a counter, about 8 KB per GPU, held until exit), so at
- * most 1024 CTAs: devices with more than 256 SMs get ISPM_ERR_TOO_LARGE.  The
- * first call on a device looks the array up (cudaGetSymbolAddress) -- make it
+ * (1024 partial sums + a counter, about 8 KB per GPU, held until exit); the
+ * dot's grid is capped at 1024 CTAs, so a device with more than 256 SMs runs
+ * it with 1024 CTAs.  The first call on a device looks the array up (cudaGetSymbolAddress) -- make it
  * before any stream capture.  All calls share the array: calls that overlap
  * on the GPU race. */
 int ispm_sblas_dot_noalloc(int dtype, const void *x, const void *y, void *s, int n,

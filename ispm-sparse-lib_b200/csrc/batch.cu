@@ -41,6 +41,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "cuda_util.cuh"
@@ -636,6 +637,10 @@ struct Batch {
       ref_h[L] = ru * ru * res_h[L];
       if (bnorm[L] == 0.0) {  // x = 0 solves it
         state[L] = kFinished, skip[L] = 1, fin[L] = 1;
+      } else if (!std::isfinite(bnorm[L])) {  // NaN / Inf in b: the lane cannot converge
+        state[L] = kFailed, skip[L] = 1, fin[L] = 1;
+        status[L] = ISPM_ERR_INVALID;
+        rel[L] = bnorm[L];
       } else {
         rel[L] = 1.0;
         active++;
@@ -1104,6 +1109,10 @@ int ispm_batch_create(int n_systems, const int *n_rows, const int *const *row_pt
   for (int k = 0; k < n_systems; k++) {
     if (n_rows[k] <= 0 || n_rhs[k] <= 0 || !row_ptr[k] || !cols[k] || !vals[k])
       return fail(ISPM_ERR_INVALID, "system %d: bad arguments", k);
+    if (int e = validate_csr(n_rows[k], n_rows[k], row_ptr[k], cols[k])) {
+      const std::string why = ispm_last_error();
+      return fail(e, "system %d: %s", k, why.c_str());
+    }
   }
   std::unique_ptr<ispm_batch> h(new (std::nothrow) ispm_batch);
   if (!h)

@@ -521,6 +521,11 @@ int check_csr(int n_rows, int n_cols, const int *row_ptr, const int *cols)
 
 }  // namespace
 
+int validate_csr(int n_rows, int n_cols, const int *row_ptr, const int *cols)
+{
+  return check_csr(n_rows, n_cols, row_ptr, cols);
+}
+
 ispm_slell_view HostSlell::view() const
 {
   ispm_slell_view v;

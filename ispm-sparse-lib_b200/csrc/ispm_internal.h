@@ -41,6 +41,10 @@ struct HostSlell {
   ispm_slell_view view() const;
 };
 
+// ISPM_ERR_INVALID unless row_ptr[0] == 0, row_ptr never decreases and every
+// column index lies in [0, n_cols).
+int validate_csr(int n_rows, int n_cols, const int *row_ptr, const int *cols);
+
 // Conversion entry used by the C ABI and the plan.
 int convert_csr(int elm_dtype, int n_rows, int n_cols, const int *row_ptr, const int *cols,
                 const void *elms, int S, int hblock, bool var_height, bool use_diags,

@@ -782,6 +782,18 @@ struct Solver {
     if (int e = true_residual(s))  // r64 = b
       return e;
     const double bnorm = std::sqrt(st_host->res2);
+    if (!std::isfinite(bnorm)) {
+      // a NaN or infinite right-hand side: no iterate can meet a relative
+      // target; stop before iterating (x stays zero)
+      ispm_solve_stats out{};
+      out.true_relres = bnorm;
+      out.converged = 0;
+      out.status = ISPM_ERR_INVALID;
+      out.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      if (stats)
+        *stats = out;
+      return fail(ISPM_ERR_INVALID, "the right-hand side holds a NaN or infinite value");
+    }
     double rel = bnorm > 0 ? 1.0 : 0.0;
     int total_it = 0, status = ISPM_OK;
     const double target = opts.tol * bnorm;
@@ -889,7 +901,10 @@ struct Solver {
       e = launched("permute b");
       if (!e)
         e = solve(b_perm, x_perm, stats, own);
-      if (!e || e == ISPM_ERR_NOT_CONVERGED || e == ISPM_ERR_BREAKDOWN) {
+      // x in the caller's order whenever solve() ran (a refused non-finite b
+      // leaves the zero iterate)
+      if (!e || e == ISPM_ERR_NOT_CONVERGED || e == ISPM_ERR_BREAKDOWN ||
+          e == ISPM_ERR_INVALID) {
         cudaError_t me = cudaMemsetAsync(x, 0, (size_t)n_pad * sizeof(double), own);
         if (me == cudaSuccess)
           permute_out_kernel<<<grid_for(n), kThreads, 0, own>>>(x, x_perm, perm, n);
@@ -1031,6 +1046,18 @@ int ispm_solver_create(int n, const int *row_ptr, const int *cols, const double 
   if (!out || n <= 0 || !row_ptr || !cols || !vals)
     return fail(ISPM_ERR_INVALID, "bad arguments");
   *out = nullptr;
+  // the reordering and the conversions index with these arrays: reject a
+  // malformed CSR before anything walks it
+  if (int e = validate_csr(n, n, row_ptr, cols))
+    return e;
+  if ((g1_rp && !g1_ci) || (g2_rp && !g2_ci))
+    return fail(ISPM_ERR_INVALID, "factor row pointers without column indices");
+  if (g1_rp)
+    if (int e = validate_csr(n, n, g1_rp, g1_ci))
+      return e;
+  if (g2_rp)
+    if (int e = validate_csr(n, n, g2_rp, g2_ci))
+      return e;
   std::unique_ptr<ispm_solver> h(new (std::nothrow) ispm_solver);
   if (!h)
     return fail(ISPM_ERR_NOMEM, "host allocation");

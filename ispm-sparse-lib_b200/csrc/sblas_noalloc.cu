@@ -11,9 +11,10 @@
 // the library until the process exits.
 //
 // Limits and sharing:
-//  * a launch uses at most 4 CTAs per SM, one partial slot each; a device with
-//    more than 256 SMs would need more than the 1024 slots and is rejected with
-//    ISPM_ERR_TOO_LARGE (the B200 uses 592);
+//  * a launch uses at most 4 CTAs per SM and never more than 1024 CTAs (the
+//    grid cap every sblas reduction shares), one partial slot each, so the
+//    1024 slots always suffice: a device with more than 256 SMs runs the dot
+//    with 1024 CTAs (the B200 uses 592);
 //  * every call shares the one array: calls whose work overlaps on the GPU
 //    (different streams or host threads) race on it and give wrong results;
 //  * the arrival counter is cleared (cudaMemsetAsync on the caller's stream)
@@ -32,6 +33,8 @@
 namespace {
 
 constexpr int kNoAllocSlots = 1024;
+static_assert(kNoAllocSlots >= ispm::kSblasMaxBlocks,
+              "the static scratch must hold a partial for every CTA sblas_grid allows");
 
 // Slots 0 .. kNoAllocSlots-1: per-CTA partial sums (doubles); the last word
 // holds the arrival counter.
@@ -72,13 +75,8 @@ int ispm_sblas_dot_noalloc(int dtype, const void *x, const void *y, void *s, int
     return fail(ISPM_ERR_INVALID, "dtype %d", dtype);
   if (n < 0 || !s || (n && (!x || !y)))
     return fail(ISPM_ERR_INVALID, "bad arguments");
-  const size_t esz = dtype == ISPM_F32 ? 4 : 8;
-  const int vec = aligned(x, 16) && aligned(y, 16);
-  const int grid = sblas_grid(n, vec ? 16 / (int)esz : 1);
-  if (grid > kNoAllocSlots)
-    return fail(ISPM_ERR_TOO_LARGE,
-                "dot needs %d partial slots, the static scratch holds %d (more than 256 SMs)",
-                grid, kNoAllocSlots);
+  // dot_launch sizes its grid with sblas_grid, which never exceeds
+  // kSblasMaxBlocks <= kNoAllocSlots (static_assert above)
   unsigned long long *base = nullptr;
   if (int st = scratch_address(&base))
     return st;

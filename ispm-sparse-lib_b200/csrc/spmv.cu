@@ -24,6 +24,7 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <type_traits>
 
 #include "cuda_util.cuh"
@@ -51,6 +52,7 @@ template <class T, class E> struct SpmvArgs {
   int pdl;            // launched as a programmatic dependent of the previous kernel
   const float *dg;    // split operators (E = __half): FP32 diagonal, one per row
   float inv_scale;    // split operators: 1 / the power-of-two element scale
+  int stage_words;    // staged walk: x staging capacity (values of T) per CTA
 };
 
 // Finish a fused dot product: every block publishes its partial, the last
@@ -554,7 +556,7 @@ __global__ void __launch_bounds__(512, sizeof(T) == 8 ? 3 : 4)
       }
     }
     __syncthreads();
-    staged = s_total <= (int)(kStageWordsPerRow * rows);
+    staged = s_total <= a.stage_words;
     if (staged) {
       const int n = (int)a.n_cols;
       const int nb = s_nb;
@@ -676,12 +678,16 @@ bool staged_shape(const ispm_launch_params &p, const ispm_slell_view &m)
 }
 
 template <class T, class E>
-int launch_staged(const SpmvArgs<T, E> &args, cudaStream_t stream)
+int launch_staged(SpmvArgs<T, E> args, cudaStream_t stream)
 {
   const unsigned rows = args.slice_height > kStageMinRows ? args.slice_height : kStageMinRows;
   const unsigned spb = rows / args.slice_height;
   const unsigned grid = (args.n_slices + spb - 1) / spb;
-  const size_t smem = (size_t)kStageWordsPerRow * rows * sizeof(T);
+  // staging buffer: kStageWordsPerRow values per row, at most 40 KB so that
+  // with the kernel's static tables it stays inside the 48 KB a launch gets
+  // without opting in to more
+  const size_t smem = std::min<size_t>((size_t)kStageWordsPerRow * rows * sizeof(T), 40960);
+  args.stage_words = (int)(smem / sizeof(T));
   cudaError_t e = launch_kernel(slell_spmv_staged_kernel<T, E>, dim3(grid), dim3(rows), smem,
                                 stream, args.pdl != 0, args);
   if (e == cudaSuccess)
@@ -761,6 +767,7 @@ int launch_te(const ispm_launch_params &p, const ispm_slell_view &m, const void 
   a.pdl = pdl ? 1 : 0;
   a.dg = nullptr;
   a.inv_scale = 1.f;
+  a.stage_words = 0;
   if constexpr (std::is_same<E, __half>::value) {
     if (!split || !split->diag || !aligned(split->diag, 16))
       return fail(ISPM_ERR_INVALID, "FP16 elements need the split operator's diagonal vector");

@@ -978,7 +978,11 @@ class BatchSolver:
         return int(_lib().ispm_batch_fsai_fallbacks(self._h))
 
     def _finish(self, rc, lanes, tot):
-        if rc not in (OK, ERR_NOT_CONVERGED, ERR_BREAKDOWN):
+        # a lane whose right-hand side holds NaN / Inf stops with ERR_INVALID
+        # in its own status; the other lanes' results stand
+        lane_invalid = any(lanes[l].status == ERR_INVALID for l in range(len(lanes)))
+        if rc not in (OK, ERR_NOT_CONVERGED, ERR_BREAKDOWN) and not (
+                rc == ERR_INVALID and lane_invalid):
             _check(rc)
         return [lanes[l].as_dict() for l in range(len(lanes))], tot.as_dict()
 

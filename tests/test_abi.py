@@ -5,6 +5,8 @@ import glob
 import os
 import re
 
+import numpy as np
+
 from conftest import PKG, ROOT
 
 
@@ -76,3 +78,38 @@ def test_solver_default_options(ispm):
     assert o.replace_ratio_f32 == 1e-2 and o.replace_ratio_f64 == 1e-4
     assert (o.variant, o.prec, o.factor_bf16, o.reorder) == (0, 0, 0, 2)
     assert o.matrix_f16 == 0
+
+
+def test_solver_rejects_malformed_csr_before_reordering(ispm, gen):
+    """ispm_solver_create and ispm_batch_create validate row_ptr and the column
+    indices before the reverse Cuthill-McKee ordering or any conversion walks
+    them (an out-of-range column used to index the ordering's work arrays).
+    No GPU needed: the check comes before any device work."""
+    import pytest
+    A = gen.poisson7(6)
+    cases = []
+    bad_col = A.cols.copy()
+    bad_col[7] = A.n_cols + 1000
+    cases.append(("column past n", A.row_ptr, bad_col))
+    neg_col = A.cols.copy()
+    neg_col[11] = -5
+    cases.append(("negative column", A.row_ptr, neg_col))
+    bad_rp = A.row_ptr.copy()
+    bad_rp[10], bad_rp[11] = bad_rp[11] + 3, bad_rp[10]
+    cases.append(("decreasing row_ptr", bad_rp, A.cols))
+    off_rp = A.row_ptr.copy() + 1
+    cases.append(("row_ptr[0] != 0", off_rp, A.cols))
+    for name, rp, ci in cases:
+        M = ispm.csr_matrix(A.n_rows, A.n_cols, rp, ci, A.elms)
+        for reorder in ("auto", "rcm", "none"):
+            with pytest.raises(ispm.IspmError) as e:
+                ispm.PCGSolver(M, inner=np.float64, prec="fsai_gpu", reorder=reorder)
+            assert e.value.status == ispm.ERR_INVALID, (name, reorder)
+        with pytest.raises(ispm.IspmError) as e:
+            ispm.BatchSolver([A, M], 1)
+        assert e.value.status == ispm.ERR_INVALID, name
+    # a malformed factor pair is refused the same way
+    with pytest.raises(ispm.IspmError) as e:
+        ispm.PCGSolver(A, ispm.csr_matrix(A.n_rows, A.n_cols, A.row_ptr, bad_col, A.elms), A,
+                       inner=np.float64)
+    assert e.value.status == ispm.ERR_INVALID

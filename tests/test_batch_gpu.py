@@ -165,3 +165,27 @@ def test_batch_single_lane_and_tiny_system(ispm, oracle, cuda, gen):
     xs2, lanes2, tot2 = B2.solve_host([np.array([2.0]), b])
     assert tot2["converged"], lanes2
     assert abs(xs2[0][0] - 0.5) <= 1e-12
+
+
+@pytest.mark.parametrize("bad", [np.nan, np.inf])
+def test_batch_non_finite_rhs_stops_only_its_lane(ispm, oracle, cuda, gen, bad):
+    """A lane whose right-hand side holds NaN / Inf stops at once with
+    ERR_INVALID in its own status; every other lane still converges."""
+    systems, n_rhs, dims = _small_batch(gen, n=4, seed=5)
+    _, bs = gen.batch_rhs(systems, n_rhs, seed=2)
+    bs = [b.copy() for b in bs]
+    bs[1].reshape(-1)[3] = bad
+    B = ispm.BatchSolver(systems, n_rhs, inner=np.float32, tol=1e-8)
+    xs, lanes, tot = B.solve_host(bs)
+    assert not tot["converged"]
+    for lane in range(B.lanes):
+        info = B.lane_info(lane)
+        k, j = info["system"], info["rhs"]
+        b = bs[k].reshape(n_rhs[k], -1)[j]
+        if not np.all(np.isfinite(b)):
+            assert lanes[lane]["status"] == ispm.ERR_INVALID and not lanes[lane]["converged"]
+            assert lanes[lane]["iterations"] == 0
+        else:
+            assert lanes[lane]["converged"], (lane, lanes[lane])
+            x = xs[k].reshape(n_rhs[k], -1)[j]
+            assert _true_rel(oracle, systems[k], x, b) <= 1e-8 * 1.001

@@ -116,9 +116,34 @@ def test_pcg_indefinite_matrix_stops(ispm, cuda):
     d = np.where(np.arange(n) % 2 == 0, 2.0, -2.0)
     rp = np.arange(n + 1, dtype=np.int32)
     A = ispm.csr_matrix(n, n, rp, np.arange(n, dtype=np.int32), d)
-    s = ispm.PCGSolver(A, None, None, inner=np.float64, tol=1e-10, max_refinements=3)
-    x, st = s.solve_host(np.ones(n))
-    assert not st["converged"] or np.allclose(x, 1.0 / d)
+    # p.Ap = sum(d) = 0 on the first step: alpha is infinite, the step is
+    # refused, and after three restarts that do not lower the residual the
+    # solver stops with ERR_BREAKDOWN
+    for inner in (np.float64, np.float32):
+        s = ispm.PCGSolver(A, None, None, inner=inner, tol=1e-10, max_refinements=5)
+        x, st = s.solve_host(np.ones(n))
+        assert not st["converged"], (inner, st)
+        assert st["status"] == ispm.ERR_BREAKDOWN, (inner, st)
+        assert np.all(np.isfinite(x)) and st["true_relres"] >= 1e-10
+
+
+@pytest.mark.parametrize("bad", [np.nan, np.inf, -np.inf])
+@pytest.mark.parametrize("inner", [np.float32, np.float64])
+def test_pcg_non_finite_rhs_is_refused(ispm, oracle, cuda, c1, bad, inner):
+    """A NaN or infinite entry in b cannot be solved to a relative target: the
+    solve returns ERR_INVALID at once (it used to report convergence with
+    x = 0, since ||b|| compared as not positive), and the solver stays usable."""
+    A, b, G1, G2 = c1
+    s = ispm.PCGSolver(A, G1, G2, inner=inner, tol=1e-10)
+    bb = b.copy()
+    bb[123] = bad
+    with pytest.raises(ispm.IspmError) as e:
+        s.solve_host(bb)
+    assert e.value.status == ispm.ERR_INVALID
+    x, st = s.solve_host(b)
+    assert st["converged"]
+    r = b - oracle.csr_spmv_f64(A.row_ptr, A.cols, A.elms, x)
+    assert np.linalg.norm(r) <= 1.001e-10 * np.linalg.norm(b)
 
 
 @pytest.mark.parametrize("inner", [np.float32, np.float64])
