@@ -72,6 +72,8 @@ def parse():
                         "FP32, or FP16 off-diagonals + corrected FP32 diagonal (matrix_f16); "
                         "the other one is timed beside it")
     p.add_argument("--reps", type=int, default=5)
+    p.add_argument("--no-extra", action="store_true",
+                   help="leave out the compact 192^3 unstructured and batched sub-results")
     p.add_argument("--workload", choices=["c2", "c3", "c4"], default="c2",
                    help="c2: the 128^3 27-point system (default); c3: the 192^3 "
                         "unstructured permuted system; c4: the batch of 96 uneven systems")
@@ -249,34 +251,37 @@ def run_reference(args, rank, world):
     Ac = (A.row_ptr, A.cols, A.elms)
     g1 = (G1.row_ptr, G1.cols, G1.elms)
     g2 = (G2.row_ptr, G2.cols, G2.elms)
-    # warm-up: one full solve fixes the iteration count the samples scale to
+    # every step is one whole host solve to the tolerance; warm-up is one
+    # solve (a CPU code has no device to warm), and the step count is cut so
+    # that the run stays within about three minutes
     t0 = time.perf_counter()
     _, iters, rel = O.pcg_f64(Ac, b, g1, g2, pipelined=True, tol=args.tol, max_it=20000)
-    full = time.perf_counter() - t0
-    log(f"[reference] full CPU solve: {iters} iterations, relres {rel:.2e}, {full:.1f}s")
+    first = time.perf_counter() - t0
+    log(f"[reference] warm-up host solve: {iters} iterations, relres {rel:.2e}, {first:.1f}s")
+    steps = max(1, min(args.steps, int(180.0 // max(first, 1e-3))))
     times = []
-    for k in range(args.warmup + args.steps):
+    for _ in range(steps):
         t0 = time.perf_counter()
-        _, it, _ = O.pcg_f64(Ac, b, g1, g2, pipelined=True, tol=1e-30,
-                             max_it=args.cpu_sample_iters)
-        dt = (time.perf_counter() - t0) / max(it, 1) * iters
-        if k >= args.warmup:
-            times.append(dt)
+        _, it, rel = O.pcg_f64(Ac, b, g1, g2, pipelined=True, tol=args.tol, max_it=20000)
+        times.append(time.perf_counter() - t0)
+        if it != iters:
+            raise RuntimeError(f"host solve took {it} iterations, the warm-up {iters}")
     v = float(np.mean(times))
     cores = O.orc().orc_num_threads()
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
-        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": WORKLOAD, "grid": args.grid,
-                                        "rows": A.n_rows, "nnz": A.n_nz, "tol": args.tol,
-                                        "l2": "inputs larger than L2"},
+        "steps": steps, "steps_requested": args.steps, "warmup": 1,
+        "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": args.grid, "rows": A.n_rows, "nnz": A.n_nz,
+                   "tol": args.tol, "l2": "inputs larger than L2"},
         "cpu_baseline": {"value": v, "unit": "s", "cores": cores, "kind": "port",
-                         "sample": f"{args.cpu_sample_iters} iterations of the host pipelined "
-                                   f"FP64 FSAI-PCG per step, scaled to the {iters} iterations "
-                                   f"of a full host solve (measured {full:.1f}s)"},
+                         "sample": f"whole host solves to {args.tol:g}: pipelined FP64 "
+                                   f"FSAI-PCG ({iters} iterations) with the reference's "
+                                   f"fastainv.cpp pair (droptol {args.droptol}, compiled in "
+                                   f"place), {steps} timed after 1 warm-up"},
         "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "iterations": iters, "true_relres": rel, "full_solve_s": full,
+        "iterations": iters, "true_relres": rel, "solve_s_each": times,
     }), flush=True)
 
 
@@ -634,6 +639,106 @@ def run_c4(args, rank, world, local):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------- compact C3 / C4
+def c3_compact(ispm, gen, torch, stream, tol, steps=3):
+    """The 192^3 unstructured permuted system, for the headline line: the
+    mixed PCG and the plain FP64 pipelined PCG (same GPU FSAI, same solver
+    renumbering), each with its worst true residual against the FP64 CSR
+    product, and the FP32 SpMV in the exhaustive plan's shape against the
+    measured copy bandwidth."""
+    t0 = time.time()
+    A = gen.unstructured(192, 0.05, 1, 0.1, 10.0, 1.01)
+    b = oracle_spmv(A, np.random.default_rng(0).uniform(-1, 1, A.n_rows))
+    A32 = ispm.csr_matrix(A.n_rows, A.n_cols, A.row_ptr, A.cols, A.elms.astype(np.float32))
+    plan = ispm.spmv_plan(A32, ispm.PLAN_EXHAUSTIVE, T=np.float32)
+    mp, lp = plan.mparams, plan.params
+    view = plan.host_matrix.view()
+    xs = torch.rand(A.n_cols, dtype=torch.float32, device="cuda")
+    ys = torch.zeros(view.n_rows, dtype=torch.float32, device="cuda")
+    for _ in range(5):
+        plan.execute_spmv(xs, ys, stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(30):
+        plan.execute_spmv(xs, ys, stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_spmv = e0.elapsed_time(e1) / 30 * 1e-3
+    alg = algorithmic_bytes(view, 4)
+    peak, _ = measured_peak()
+    del plan
+    out = {"workload": C3_WORKLOAD, "rows": A.n_rows, "nnz": A.n_nz, "tol": tol,
+           "spmv": {"S": mp.S, "hblock": mp.H, "var_height": mp.V, "diags": mp.D, "N": lp.N,
+                    "H": lp.H, "us": t_spmv * 1e6, "algorithmic_bytes": alg,
+                    "achieved_gbs": alg / t_spmv / 1e9, "frac": alg / t_spmv / 1e9 / peak}}
+    for name, kw in (("mixed", dict(inner=np.float32)),
+                     ("plain_fp64", dict(inner=np.float64, variant="pipelined"))):
+        S = ispm.PCGSolver(A, tol=tol, prec="fsai_gpu", **kw)
+        bd = torch.zeros(S.rows, dtype=torch.float64, device="cuda")
+        bd[: A.n_rows] = torch.from_numpy(b).cuda()
+        xd = torch.zeros_like(bd)
+        S.solve(bd, xd, stream)
+        ms = []
+        for _ in range(steps):
+            ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ea.record(stream)
+            st = S.solve(bd, xd, stream)
+            eb.record(stream)
+            torch.cuda.synchronize()
+            ms.append(ea.elapsed_time(eb))
+        x = xd[: A.n_rows].cpu().numpy()
+        out[name] = {"solve_s": float(np.mean(ms)) * 1e-3, "iterations": st["iterations"],
+                     "converged": bool(st["converged"]),
+                     "true_relres": float(np.linalg.norm(b - oracle_spmv(A, x)) /
+                                          np.linalg.norm(b))}
+        del S
+    out["speedup_vs_plain_fp64"] = out["plain_fp64"]["solve_s"] / out["mixed"]["solve_s"]
+    out["wall_s"] = time.time() - t0
+    log(f"[c3] {out}")
+    return out
+
+
+def c4_compact(ispm, gen, torch, stream, steps=3):
+    """The 96-system batch (260 right-hand sides) to 1e-8, for the headline
+    line: batched solve time, iterations and the worst lane's true residual
+    against the FP64 CSR product."""
+    t0 = time.time()
+    systems, n_rhs, dims = gen.batch_systems(96, seed=0)
+    _, bs = gen.batch_rhs(systems, n_rhs, seed=0)
+    B = ispm.BatchSolver(systems, n_rhs, inner=np.float32, tol=1e-8)
+    bh = np.zeros(B.rows)
+    infos = [B.lane_info(l) for l in range(B.lanes)]
+    for info in infos:
+        bb = bs[info["system"]][info["rhs"]]
+        bh[info["row0"]:info["row0"] + bb.size] = bb
+    bd = torch.tensor(bh, device="cuda")
+    xd = torch.zeros_like(bd)
+    B.solve(bd, xd, stream)
+    ms = []
+    for _ in range(steps):
+        ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ea.record(stream)
+        lanes, tot = B.solve(bd, xd, stream)
+        eb.record(stream)
+        torch.cuda.synchronize()
+        ms.append(ea.elapsed_time(eb))
+    xh = xd.cpu().numpy()
+    worst = 0.0
+    for info in infos:
+        A = systems[info["system"]]
+        bb = bs[info["system"]][info["rhs"]]
+        x = xh[info["row0"]:info["row0"] + A.n_rows]
+        worst = max(worst, float(np.linalg.norm(bb - oracle_spmv(A, x)) / np.linalg.norm(bb)))
+    its = [l["iterations"] for l in lanes]
+    out = {"workload": C4_WORKLOAD, "systems": len(systems), "lanes": B.lanes,
+           "solve_s": float(np.mean(ms)) * 1e-3, "converged": bool(tot["converged"]),
+           "iterations_max": int(max(its)), "iterations_mean": float(np.mean(its)),
+           "true_relres_max": worst, "wall_s": time.time() - t0}
+    del B
+    log(f"[c4] {out}")
+    return out
+
+
 # ---------------------------------------------------------------- our arm
 def main():
     args = parse()
@@ -686,6 +791,10 @@ def main():
     t0 = time.time()
     mixed = ispm.PCGSolver(A, G1, G2, inner=np.float32, tol=args.tol)
     plain = ispm.PCGSolver(A, G1, G2, inner=np.float64, tol=args.tol)
+    # plain FP64 pipelined PCG with the headline's own factor (GPU FSAI): the
+    # precision change alone, the preconditioner held fixed
+    plain_fsai = ispm.PCGSolver(A, None, None, inner=np.float64, tol=args.tol, prec="fsai_gpu",
+                                variant="pipelined")
     log(f"[setup] GPU FSAI solver {t_setup:.1f}s, AINV solvers {time.time() - t0:.1f}s")
     # learned per-row drop tolerances (the trained network's prediction fed to
     # fastainv_sym_ex), judged against the plain build by the gate
@@ -741,10 +850,12 @@ def main():
         alt.solve(bd, xd, stream)
         mixed.solve(bd, xd, stream)
         plain.solve(bd, xd, stream)
+        plain_fsai.solve(bd, xd, stream)
         learned.solve(bd, xd, stream)
     ms_alt, st_alt = timed(alt, k_side, "mixed+GPU FSAI, other matrix storage")
     ms_mixed, st_mixed = timed(mixed, k_side, "mixed+AINV")
     ms_plain, st_plain = timed(plain, k_side, "plain FP64+AINV")
+    ms_pfsai, st_pfsai = timed(plain_fsai, k_side, "plain FP64+GPU FSAI")
     ms_learned, st_learned = timed(learned, k_side, "mixed+learned AINV")
     del mixed, learned, alt
 
@@ -801,11 +912,39 @@ def main():
     t_plain = float(np.mean(ms_plain)) * 1e-3
     t_learned = float(np.mean(ms_learned)) * 1e-3
     t_alt = float(np.mean(ms_alt)) * 1e-3
+    t_pfsai = float(np.mean(ms_pfsai)) * 1e-3
     if world > 1:
-        tt = torch.tensor([t_best, e2e, t_mixed, t_plain, t_learned, t_alt],
+        tt = torch.tensor([t_best, e2e, t_mixed, t_plain, t_learned, t_alt, t_pfsai],
                           dtype=torch.float64, device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_best, e2e, t_mixed, t_plain, t_learned, t_alt = tt.tolist()
+        t_best, e2e, t_mixed, t_plain, t_learned, t_alt, t_pfsai = tt.tolist()
+
+    # iteration rooflines: compulsory bytes of one iteration (the three
+    # SpMVs' algorithmic bytes plus the vector passes outside them) x
+    # iterations / solve time, against the measured copy bandwidth.  Classic
+    # mixed iteration: 11 FP32 vector passes beyond the SpMVs' x and y
+    # (p.q epilogue 1, update 6, r.z/r.r epilogue 1, direction 3); pipelined
+    # FP64 iteration: the fused update's 18 FP64 passes.
+    n = A.n_rows
+    Gf1, Gf2 = ispm.fsai_sym_gpu(A, np.float64)
+
+    def spmv_alg(M, dt):
+        Mc = ispm.csr_matrix(M.n_rows, M.n_cols, M.row_ptr, M.cols,
+                             np.asarray(M.elms).astype(dt))
+        return algorithmic_bytes(ispm.csr_to_slell_guess_format(Mc).view(), np.dtype(dt).itemsize)
+
+    a32, a64 = spmv_alg(A, np.float32), spmv_alg(A, np.float64)
+    bytes_it = {
+        "mixed_fsai_gpu": a32 + spmv_alg(Gf1, np.float32) + spmv_alg(Gf2, np.float32) + 11 * 4 * n,
+        "plain_fp64_ainv": a64 + spmv_alg(G1, np.float64) + spmv_alg(G2, np.float64) + 18 * 8 * n,
+        "plain_fp64_fsai_gpu": a64 + spmv_alg(Gf1, np.float64) + spmv_alg(Gf2, np.float64)
+                               + 18 * 8 * n}
+    del Gf1, Gf2
+
+    def it_roof(key, t, st):
+        ach = bytes_it[key] * st["iterations"] / t / 1e9
+        return {"bytes_per_iteration": bytes_it[key], "achieved_gbs": ach,
+                "frac": ach / peak, "peak_gbs": peak}
     it_l, it_m = st_learned[-1]["iterations"], st_mixed[-1]["iterations"]
 
     # classic FP32 iteration: A SpMV (+p.Ap), r/x update, G SpMV, G^T SpMV
@@ -845,7 +984,17 @@ def main():
                            "nnz_G": G1.n_nz, "droptol": args.droptol,
                            "fastainv_host_s": t_ainv},
             "plain_fp64_ainv": {"solve_s": t_plain, "iterations": st_plain[-1]["iterations"],
-                                "method": "pipelined FP64 PCG, fastainv droptol 0.01"},
+                                "method": "pipelined FP64 PCG, fastainv droptol 0.01",
+                                "iteration_roofline": it_roof("plain_fp64_ainv", t_plain,
+                                                              st_plain[-1])},
+            "plain_fp64_fsai_gpu": {"solve_s": t_pfsai,
+                                    "iterations": st_pfsai[-1]["iterations"],
+                                    "method": "pipelined FP64 PCG with the headline's GPU FSAI "
+                                              "factor (precision changed, factor held fixed)",
+                                    "iteration_roofline": it_roof("plain_fp64_fsai_gpu",
+                                                                  t_pfsai, st_pfsai[-1])},
+            "speedup_vs_plain_fp64_same_factor": t_pfsai / t_best,
+            "iteration_roofline": it_roof("mixed_fsai_gpu", t_best, st_best[-1]),
             "learned_mixed_ainv": {
                 "solve_s": t_learned, "iterations": it_l, "nnz_G": L1.n_nz,
                 "droptol_median": float(np.median(l_tau)), "predict_s": t_pred,
@@ -869,6 +1018,11 @@ def main():
             "cpu_baseline": cpu,
             "device": dev_name,
         }
+        if world == 1 and not args.no_extra:
+            del best, plain, plain_fsai
+            torch.cuda.empty_cache()
+            out["c3"] = c3_compact(ispm, gen, torch, stream, args.tol)
+            out["c4"] = c4_compact(ispm, gen, torch, stream)
         print(json.dumps(out), flush=True)
     if world > 1:
         dist.destroy_process_group()

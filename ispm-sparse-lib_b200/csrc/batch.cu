@@ -412,6 +412,7 @@ struct Batch {
   int chunk = 16;
   int graph_nodes = 0;  // kernels in one replay of the chunk graph
   int launches = 0;  // kernels launched by the last solve (graph nodes counted)
+  bool completed = false;  // the last solve ran to its end (lane results are valid)
   bool verbose = getenv("ISPM_SOLVER_VERBOSE") && atoi(getenv("ISPM_SOLVER_VERBOSE")) > 0;
 
   ~Batch()
@@ -613,6 +614,7 @@ struct Batch {
   {
     auto t0 = std::chrono::steady_clock::now();
     launches = 0;
+    completed = false;
     const int n = n_lanes;
     int *state = ib_h, *skip = ib_h + n, *fin = ib_h + 2 * n, *fresh = ib_h + 3 * n,
         *its = ib_h + 4 * n;
@@ -733,6 +735,7 @@ struct Batch {
       total->true_relres = max_rel;
       total->seconds = secs;
     }
+    completed = true;
     if (worst)
       return fail(worst, "batched solve: some lanes stopped above the tolerance (worst %.3e)",
                   max_rel);
@@ -1209,7 +1212,9 @@ int ispm_batch_solve_host(ispm_batch *b, const double *const *b_host, double *co
   ISPM_CUDA_TRY(cudaMemcpyAsync(B.b_stage, B.hb, sizeof(double) * B.n_stack,
                                 cudaMemcpyHostToDevice, st));
   int e = B.solve_on(B.b_stage, B.x_stage, lane_stats, total, st);
-  if (e && e != ISPM_ERR_NOT_CONVERGED && e != ISPM_ERR_BREAKDOWN)
+  // a completed solve hands back every lane's x, also when some lanes
+  // stopped (not converged, breakdown, a NaN / Inf right-hand side)
+  if (e && !B.completed)
     return e;
   ISPM_CUDA_TRY(cudaMemcpyAsync(B.hx, B.x_stage, sizeof(double) * B.n_stack,
                                 cudaMemcpyDeviceToHost, st));
