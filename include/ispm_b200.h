@@ -377,6 +377,12 @@ typedef struct {
                            to at least 3e-2 (a reliable update at least every
                            33x fall of the recursive residual).  A and its
                            reliable-update residuals stay FP64. */
+  int factor_f16;       /* FP32 inner solve with prec = ISPM_PREC_FSAI_GPU: keep
+                           the factor's values in FP16 times one power-of-two
+                           scale (the largest magnitude lands in [2^13, 2^14)),
+                           11 mantissa bits where BF16 keeps 8; half the bytes
+                           of each factor application.  Takes precedence over
+                           factor_bf16. */
 } ispm_solver_opts;
 
 #define ISPM_REORDER_NONE 0

@@ -1,5 +1,6 @@
 // Device initialisation and device-resident sliced-ELL matrices.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -213,9 +214,71 @@ int refresh_values_gather(DeviceSlell &d, const int *inv, const void *vals, int 
                           : fail(ISPM_ERR_CUDA, "value refresh: %s", cudaGetErrorString(e));
 }
 
+// elms[map[k]] = FP16(vals[k] * scale), rounded to nearest.
+__global__ void refresh_f16_kernel(__half *__restrict__ elms, const unsigned *__restrict__ map,
+                                   const double *__restrict__ vals, long long n, double scale)
+{
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x)
+    elms[__ldcs(map + k)] = __double2half(__ldcs(vals + k) * scale);
+}
+
+// *out = max |v_k| as the bit pattern of a non-negative double (which orders
+// like an unsigned integer); *out must start at 0.
+__global__ void absmax_kernel(const double *__restrict__ v, long long n, unsigned long long *out)
+{
+  double m = 0.0;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x)
+    m = fmax(m, fabs(v[k]));
+  for (int off = 16; off > 0; off >>= 1)
+    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+  if ((threadIdx.x & 31) == 0)
+    atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+int device_absmax(const double *vals, long long n, double &out)
+{
+  out = 0.0;
+  if (!n)
+    return ISPM_OK;
+  unsigned long long *d = nullptr;
+  ISPM_CUDA_TRY(cudaMalloc(&d, sizeof(unsigned long long)));
+  unsigned long long h = 0;
+  cudaError_t e = cudaMemset(d, 0, sizeof(h));
+  if (e == cudaSuccess) {
+    const long long blocks = std::min<long long>((n + 255) / 256, (long long)device_sm_count() * 8);
+    absmax_kernel<<<blocks, 256>>>(vals, n, d);
+    e = cudaPeekAtLastError();
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpy(&h, d, sizeof(h), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess)
+    return fail(ISPM_ERR_CUDA, "absolute maximum: %s", cudaGetErrorString(e));
+  std::memcpy(&out, &h, sizeof(out));
+  return ISPM_OK;
+}
+
+int refresh_values_f16(DeviceSlell &d, const unsigned *map, const double *vals, long long n,
+                       double scale, cudaStream_t s)
+{
+  if (d.meta.elm_dtype != ISPM_F16)
+    return fail(ISPM_ERR_INVALID, "scaled FP16 refresh of an element type %d", d.meta.elm_dtype);
+  if (!n)
+    return ISPM_OK;
+  const long long blocks = std::min<long long>((n + 255) / 256, (long long)device_sm_count() * 8);
+  refresh_f16_kernel<<<blocks, 256, 0, s>>>((__half *)d.elms, map, vals, n, scale);
+  cudaError_t e = cudaPeekAtLastError();
+  return e == cudaSuccess ? ISPM_OK
+                          : fail(ISPM_ERR_CUDA, "value refresh: %s", cudaGetErrorString(e));
+}
+
 int refresh_values(DeviceSlell &d, const unsigned *map, const void *vals, int val_dtype,
                    long long n, cudaStream_t s)
 {
+  if (d.meta.elm_dtype == ISPM_F16)
+    return fail(ISPM_ERR_INVALID, "FP16 elements are refreshed with their scale");
   if (!n)
     return ISPM_OK;
   const int threads = 256;

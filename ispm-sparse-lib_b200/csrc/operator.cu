@@ -73,7 +73,8 @@ int choose_format(int elm_dtype, int n_rows, int n_cols, const int *rp, const in
 
 int Operator::upload(int vec_dtype, int elm_dtype, int n, const int *rp, const int *ci,
                      const double *v, const ispm_slell_params *force,
-                     std::vector<unsigned> *value_pos, bool fixed_height, bool bf16_values)
+                     std::vector<unsigned> *value_pos, bool fixed_height, bool bf16_values,
+                     bool f16_values)
 {
   std::vector<float> vf;
   const void *vals = typed_values(elm_dtype, v, (size_t)rp[n], vf);
@@ -104,8 +105,14 @@ int Operator::upload(int vec_dtype, int elm_dtype, int n, const int *rp, const i
   if (value_pos)
     if (int st = value_map(best, n, rp, ci, *value_pos))
       return st;
-  if (int st = dev.upload(best, bf16_values && elm_dtype == ISPM_F32))
+  if (f16_values && elm_dtype == ISPM_F32) {
+    if (int st = dev.upload_f16(best))
+      return st;
+    diag = nullptr;
+    inv_scale = 1.f;
+  } else if (int st = dev.upload(best, bf16_values && elm_dtype == ISPM_F32)) {
     return st;
+  }
   lp = default_launch(vec_dtype, dev.view());
   return ISPM_OK;
 }

@@ -36,9 +36,9 @@ struct Operator {
   DeviceSlell dev;
   ispm_launch_params lp{};
   ispm_slell_params fmt{};
-  // Split operators (upload_split_f16): FP16 off-diagonal elements times
-  // 1 / inv_scale, plus this FP32 diagonal (device, dev.meta.n_rows entries,
-  // owned by diag_mem).
+  // FP16 elements hold the values times 1 / inv_scale.  Split operators
+  // (upload_split_f16) add this FP32 diagonal (device, dev.meta.n_rows
+  // entries, owned by diag_mem); FP16-stored factors have none.
   std::shared_ptr<float> diag_mem;
   float *diag = nullptr;
   float inv_scale = 1.f;
@@ -47,10 +47,13 @@ struct Operator {
   // min-bytes shape, or in `force`.  value_pos: CSR entry -> element slot,
   // for values computed later on the device.
   // bf16_values: keep the FP32 elements as BF16 on the device.
+  // f16_values: FP16 element storage for values written later on the device
+  // (set_f16_values); the uploaded values must be exact binary16 values
+  // (the solver passes zeros).
   int upload(int vec_dtype, int elm_dtype, int n, const int *rp, const int *ci,
              const double *v, const ispm_slell_params *force = nullptr,
              std::vector<unsigned> *value_pos = nullptr, bool fixed_height = false,
-             bool bf16_values = false);
+             bool bf16_values = false, bool f16_values = false);
   // Upload the FP16 split of an n x n FP64 CSR (split_f16): the off-diagonal
   // entries in the min-bytes sliced-ELL shape with FP16 elements, the
   // corrected diagonal as an FP32 vector.  FP32 vectors only.
@@ -58,7 +61,7 @@ struct Operator {
   int apply(int vdt, const void *x, void *y, cudaStream_t s, const int *skip,
             const SpmvDot *ep = nullptr, bool pdl = false) const
   {
-    if (diag) {
+    if (dev.meta.elm_dtype == ISPM_F16) {
       SpmvSplit sp{diag, inv_scale};
       return launch_spmv(vdt, lp, dev.view(), x, y, s, skip, ep, pdl, &sp);
     }

@@ -967,12 +967,13 @@ int build_fsai_on_device(Solver &S, int n, const int *rp, const int *ci, const d
   fsai_transpose_pattern(n, g_rp, g_ci, t_rp, t_ci, t_of);
   const size_t nnz_a = (size_t)rp[n], nnz_g = g_ci.size();
   std::vector<double> zeros(nnz_g, 0.0);  // structure only; values come from the GPU
-  const bool bf16 = S.inner == ISPM_F32 && S.opts.factor_bf16;
+  const bool f16 = S.inner == ISPM_F32 && S.opts.factor_f16;
+  const bool bf16 = S.inner == ISPM_F32 && S.opts.factor_bf16 && !f16;
   if (int e = S.G.upload(S.inner, S.inner, n, g_rp.data(), g_ci.data(), zeros.data(), nullptr,
-                         &pos_g, false, bf16))
+                         &pos_g, false, bf16, f16))
     return e;
   if (int e = S.Ht.upload(S.inner, S.inner, n, t_rp.data(), t_ci.data(), zeros.data(), nullptr,
-                          &pos_t, false, bf16))
+                          &pos_t, false, bf16, f16))
     return e;
   DevMem tmp;
   int *a_rp_d, *a_ci_d, *g_rp_d;
@@ -1003,10 +1004,29 @@ int build_fsai_on_device(Solver &S, int n, const int *rp, const int *ci, const d
   const int blocks = grid_for((long long)nnz_g);
   scatter_kernel<<<blocks, kThreads>>>(gt_v_d, t_of_d, g_v_d, (long long)nnz_g);
   ISPM_CUDA_TRY(cudaPeekAtLastError());
-  if (int e = refresh_values(S.G.dev, pos_g_d, g_v_d, ISPM_F64, (long long)nnz_g, 0))
-    return e;
-  if (int e = refresh_values(S.Ht.dev, pos_t_d, gt_v_d, ISPM_F64, (long long)nnz_g, 0))
-    return e;
+  if (f16) {
+    // one power-of-two scale for both factors: the largest magnitude lands
+    // in [2^13, 2^14), below the binary16 maximum (65504)
+    double amax = 0.0;
+    if (int e = device_absmax(g_v_d, (long long)nnz_g, amax))
+      return e;
+    int ex = 0;
+    if (amax > 0.0)
+      std::frexp(amax, &ex);
+    const double sc = std::ldexp(1.0, amax > 0.0 ? 14 - ex : 0);
+    if (!(sc > 0.0) || !std::isfinite(sc) || sc > 0x1p126 || sc < 0x1p-126)
+      return fail(ISPM_ERR_INVALID, "FP16 factor: magnitudes out of the FP32 scale range");
+    if (int e = refresh_values_f16(S.G.dev, pos_g_d, g_v_d, (long long)nnz_g, sc, 0))
+      return e;
+    if (int e = refresh_values_f16(S.Ht.dev, pos_t_d, gt_v_d, (long long)nnz_g, sc, 0))
+      return e;
+    S.G.inv_scale = S.Ht.inv_scale = (float)(1.0 / sc);
+  } else {
+    if (int e = refresh_values(S.G.dev, pos_g_d, g_v_d, ISPM_F64, (long long)nnz_g, 0))
+      return e;
+    if (int e = refresh_values(S.Ht.dev, pos_t_d, gt_v_d, ISPM_F64, (long long)nnz_g, 0))
+      return e;
+  }
   ISPM_CUDA_TRY(cudaMemcpy(&S.fsai_fallbacks, fb_d, sizeof(unsigned), cudaMemcpyDeviceToHost));
   return ISPM_OK;
 }
@@ -1035,6 +1055,7 @@ void ispm_solver_default_opts(ispm_solver_opts *o)
   o->factor_bf16 = 0;
   o->reorder = ISPM_REORDER_AUTO;
   o->matrix_f16 = 0;
+  o->factor_f16 = 0;
 }
 
 int ispm_solver_create(int n, const int *row_ptr, const int *cols, const double *vals,

@@ -380,12 +380,19 @@ __device__ __forceinline__ void spmv_body(const SpmvArgs<T, E> &a)
     }
   }
   if constexpr (std::is_same<E, __half>::value) {
-    // split operator: y = inv_scale * (stored off-diagonal sum) + diag * x
+    // FP16 elements: y = inv_scale * (stored sum), plus diag * x for a
+    // split operator
     if (active && t < R) {
-      const Vec<H, float> dv = ld_stream<H>(a.dg + y0 + t * H);
+      if (a.dg) {
+        const Vec<H, float> dv = ld_stream<H>(a.dg + y0 + t * H);
 #pragma unroll
-      for (int h = 0; h < H; h++)
-        acc[h] = fma(dv.v[h], ld_x_guard(xp, y0 + t * H + h, a.n_cols), acc[h] * a.inv_scale);
+        for (int h = 0; h < H; h++)
+          acc[h] = fma(dv.v[h], ld_x_guard(xp, y0 + t * H + h, a.n_cols), acc[h] * a.inv_scale);
+      } else {
+#pragma unroll
+        for (int h = 0; h < H; h++)
+          acc[h] *= a.inv_scale;
+      }
     }
   }
   if (active && t < R)
@@ -649,7 +656,8 @@ __global__ void __launch_bounds__(512, sizeof(T) == 8 ? 3 : 4)
   const unsigned row = b0 * S + tid;
   if constexpr (std::is_same<E, __half>::value) {
     if (active)
-      acc = fma(__ldcs(a.dg + row), ld_x_guard(a.x, row, a.n_cols), acc * a.inv_scale);
+      acc = a.dg ? fma(__ldcs(a.dg + row), ld_x_guard(a.x, row, a.n_cols), acc * a.inv_scale)
+                 : acc * a.inv_scale;
   }
   if (active)
     a.y[row] = acc;
@@ -769,8 +777,9 @@ int launch_te(const ispm_launch_params &p, const ispm_slell_view &m, const void 
   a.inv_scale = 1.f;
   a.stage_words = 0;
   if constexpr (std::is_same<E, __half>::value) {
-    if (!split || !split->diag || !aligned(split->diag, 16))
-      return fail(ISPM_ERR_INVALID, "FP16 elements need the split operator's diagonal vector");
+    if (!split || (split->diag && !aligned(split->diag, 16)))
+      return fail(ISPM_ERR_INVALID,
+                  "FP16 elements need their scale (and a 16-byte aligned split diagonal)");
     a.dg = split->diag;
     a.inv_scale = split->inv_scale;
   }

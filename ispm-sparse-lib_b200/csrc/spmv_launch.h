@@ -53,10 +53,11 @@ struct SpmvLanes {
   const int *cta_cnt = nullptr;
 };
 
-// Split operator (FP16 off-diagonal elements, elm_dtype ISPM_F16): the launch
-// computes y_i = inv_scale * (sum of the stored entries of row i times x) +
-// diag[i] * x[i], with diag holding one FP32 value per (padded) row, 0 past
-// n_cols.
+// FP16 elements (elm_dtype ISPM_F16) stored times a power of two: the launch
+// computes y_i = inv_scale * (sum of the stored entries of row i times x),
+// plus diag[i] * x[i] for a split operator (FP16 off-diagonal elements and
+// an FP32 diagonal, one value per padded row, 0 past n_cols); diag NULL: no
+// diagonal term (an FP16-stored factor).
 struct SpmvSplit {
   const float *diag = nullptr;
   float inv_scale = 1.f;
@@ -117,6 +118,11 @@ int refresh_values_gather(DeviceSlell &d, const int *inv, const void *vals, int 
                           cudaStream_t s);
 int refresh_values(DeviceSlell &d, const unsigned *map, const void *vals, int val_dtype,
                    long long n, cudaStream_t s);
+// FP16 elements: d.elms[map[k]] = FP16(vals[k] * scale) (nearest).
+int refresh_values_f16(DeviceSlell &d, const unsigned *map, const double *vals, long long n,
+                       double scale, cudaStream_t s);
+// out = max |vals[k]| over n device values (synchronous).
+int device_absmax(const double *vals, long long n, double &out);
 
 }  // namespace ispm
 

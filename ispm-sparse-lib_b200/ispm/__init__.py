@@ -655,7 +655,8 @@ class solver_opts(C.Structure):
                 ("max_refinements", C.c_int), ("check_every", C.c_int),
                 ("use_graph", C.c_int), ("replace_ratio_f32", C.c_double),
                 ("replace_ratio_f64", C.c_double), ("variant", C.c_int), ("prec", C.c_int),
-                ("factor_bf16", C.c_int), ("reorder", C.c_int), ("matrix_f16", C.c_int)]
+                ("factor_bf16", C.c_int), ("reorder", C.c_int), ("matrix_f16", C.c_int),
+                ("factor_f16", C.c_int)]
 
 
 class solve_stats(C.Structure):
@@ -709,7 +710,7 @@ class PCGSolver:
                  check_every: int = 16, use_graph: bool = True,
                  replace_ratio: float | None = None, variant: str = "auto",
                  prec: str = "given", factor_bf16: bool = False, reorder: str = "auto",
-                 matrix_f16: bool = False):
+                 matrix_f16: bool = False, factor_f16: bool = False):
         _declare_solver()
         L = _lib()
         o = solver_opts()
@@ -724,6 +725,7 @@ class PCGSolver:
         o.factor_bf16 = int(factor_bf16)
         o.reorder = {"none": 0, "rcm": 1, "auto": 2}[reorder]
         o.matrix_f16 = int(matrix_f16)
+        o.factor_f16 = int(factor_f16)
         if A.elms.dtype != np.float64:
             raise TypeError("the solver takes the FP64 matrix")
         self._keep = [A, G1, G2]
