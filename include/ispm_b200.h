@@ -124,6 +124,17 @@ void ispm_slell_free(ispm_slell *m);
 /* slell_matrix<E, device> copy constructor (formats/formats.h:56-66): upload
  * a host matrix to the current device. */
 int ispm_dslell_upload(const ispm_slell *h, ispm_dslell **out);
+/* The same for a host matrix whose FP32 elements are all exact binary16
+ * values (an FP16 split, ispm_csr_split_f16): the device copy keeps them as
+ * FP16 (elm_dtype ISPM_F16), for ispm_launch_spmv_split.  No counterpart in
+ * the reference. */
+int ispm_dslell_upload_f16(const ispm_slell *h, ispm_dslell **out);
+/* Diagnostics of the staged SpMV walk (launch shape N = S, H = 1; no
+ * counterpart in the reference): the tile records an upload of m computes
+ * (96 ints per 1024-row tile; none unless m has diagonal blocks and a fixed
+ * slice height dividing 1024).  *n_ints receives the count; at most cap ints
+ * are written to out (which may be NULL with cap 0). */
+int ispm_slell_stage_records(const ispm_slell *m, int *out, long long cap, long long *n_ints);
 /* Re-upload only the element values of a matrix with unchanged structure
  * (plan/plan.h:39-42, implemented as the element-only H2D copy it means). */
 int ispm_dslell_update_elms(ispm_dslell *d, const ispm_slell *h);

@@ -44,8 +44,145 @@ static uint16_t to_bf16(float f)
   return (uint16_t)(u >> 16);
 }
 
+// ---- staged-walk tile records ----------------------------------------------
+
+void stage_records(const HostSlell &h, std::vector<int> &rec)
+{
+  rec.clear();
+  const unsigned S = h.slice_height;
+  if (!h.diags || h.var_height || h.hblock != 1 || !S || kStageTileRows % S || !h.n_slices)
+    return;
+  const unsigned spt = kStageTileRows / S;
+  const unsigned n_tiles = (h.n_slices + spt - 1) / spt;
+  rec.assign((size_t)n_tiles * kStageRecInts, 0);
+  const unsigned *sp = h.slice_ptr.data();
+  // slice b: [elms_end, cols_end, diag_ptr] at 3b (conversion.h:393-402)
+  auto n_diag = [&](unsigned b) {
+    const unsigned e0 = sp[3 * b], c0 = sp[3 * b + 1], e1 = sp[3 * b + 3], c1 = sp[3 * b + 4];
+    return (int)((e1 - e0 - (c1 - c0)) / S);
+  };
+  const long long rows = kStageTileRows;
+  for (unsigned t = 0; t < n_tiles; t++) {
+    int *r = rec.data() + (size_t)t * kStageRecInts;
+    const unsigned b0 = t * spt, nsl = std::min(spt, h.n_slices - b0);
+    const int nd0 = n_diag(b0);
+    const unsigned dd0 = sp[3 * b0 + 2];
+    bool uniform = nd0 >= 1 && nd0 <= kStageMaxDiag;
+    for (unsigned s = 1; s < nsl && uniform; s++) {
+      const unsigned b = b0 + s, dd = sp[3 * b + 2];
+      if (n_diag(b) != nd0) {
+        uniform = false;
+        break;
+      }
+      for (int k = 0; k < nd0 && uniform; k++)
+        uniform = sp[dd + k] - s * S == sp[dd0 + k];
+    }
+    if (!uniform)
+      continue;  // r[0] = 0: the tile reads x directly
+    // runs of ascending window starts less than rows + gap apart share a band
+    long long lo[kStageMaxDiag], hi[kStageMaxDiag];
+    int band[kStageMaxDiag], nb = 0;
+    for (int k = 0; k < nd0; k++) {
+      const long long w = (long long)sp[dd0 + k] - S;
+      const long long wp = k ? (long long)sp[dd0 + k - 1] - S : 0;
+      if (k == 0 || w < wp || w - wp > rows + kStageGap) {
+        lo[nb] = w;
+        nb++;
+      }
+      hi[nb - 1] = w + rows;
+      band[k] = nb - 1;
+    }
+    if (nb > kStageMaxBands)
+      continue;
+    // shared-memory placement: column c sits at a word congruent to c
+    // modulo 4, so 16-byte chunks of x (FP32 or FP64) land on 16-byte chunks
+    long long off = 0, offs[kStageMaxBands];
+    for (int q = 0; q < nb; q++) {
+      off = (off + 3) / 4 * 4 + (((lo[q] % 4) + 4) % 4);
+      offs[q] = off;
+      off += hi[q] - lo[q];
+    }
+    const long long total = (off + 3) / 4 * 4;
+    if (total > (1 << 20) || lo[0] < INT32_MIN / 2 || hi[nb - 1] > INT32_MAX / 2)
+      continue;
+    r[0] = 1;
+    r[1] = nb;
+    r[2] = (int)total;
+    r[3] = nd0;
+    for (int q = 0; q < nb; q++) {
+      r[4 + 3 * q] = (int)lo[q];
+      r[5 + 3 * q] = (int)hi[q];
+      r[6 + 3 * q] = (int)offs[q];
+    }
+    for (int k = 0; k < nd0; k++) {
+      const int q = band[k];
+      r[28 + k] = (int)(offs[q] + ((long long)sp[dd0 + k] - S - lo[q]));
+    }
+  }
+}
+
+namespace {
+struct StageEntry {
+  const int *rec;
+  int max_words;
+  unsigned n_slices;
+};
+std::mutex g_stage_mu;
+std::vector<std::pair<const unsigned *, StageEntry>> g_stage;  // few live matrices
+}  // namespace
+
+bool find_stage_records(const unsigned *slice_ptr, unsigned n_slices, StageInfo &out)
+{
+  std::lock_guard<std::mutex> g(g_stage_mu);
+  for (const auto &e : g_stage)
+    if (e.first == slice_ptr && e.second.n_slices == n_slices) {
+      out.rec = e.second.rec;
+      out.max_words = e.second.max_words;
+      return true;
+    }
+  return false;
+}
+
+int DeviceSlell::attach_stage_records(const HostSlell &h)
+{
+  std::vector<int> rec;
+  stage_records(h, rec);
+  if (rec.empty())
+    return ISPM_OK;
+  int mx = 0;
+  for (size_t t = 0; t < rec.size(); t += kStageRecInts)
+    if (rec[t])
+      mx = std::max(mx, rec[t + 2]);
+  cudaError_t e = cudaMalloc(&stage_rec, rec.size() * sizeof(int));
+  if (e != cudaSuccess) {
+    stage_rec = nullptr;
+    cudaGetLastError();
+    return fail(e == cudaErrorMemoryAllocation ? ISPM_ERR_NOMEM : ISPM_ERR_CUDA,
+                "cudaMalloc(stage records): %s", cudaGetErrorString(e));
+  }
+  ISPM_CUDA_TRY(cudaMemcpy(stage_rec, rec.data(), rec.size() * sizeof(int),
+                           cudaMemcpyHostToDevice));
+  stage_max_words = mx;
+  std::lock_guard<std::mutex> g(g_stage_mu);
+  g_stage.push_back({slice_ptr, StageEntry{stage_rec, mx, meta.n_slices}});
+  return ISPM_OK;
+}
+
 void DeviceSlell::release()
 {
+  if (stage_rec) {
+    {
+      std::lock_guard<std::mutex> g(g_stage_mu);
+      for (size_t k = 0; k < g_stage.size(); k++)
+        if (g_stage[k].second.rec == stage_rec) {
+          g_stage.erase(g_stage.begin() + (long)k);
+          break;
+        }
+    }
+    cudaFree(stage_rec);
+    stage_rec = nullptr;
+    stage_max_words = 0;
+  }
   if (slice_ptr)
     cudaFree(slice_ptr);
   if (cols)
@@ -96,7 +233,7 @@ int DeviceSlell::upload(const HostSlell &h, bool bf16_values)
     ISPM_CUDA_TRY(
         cudaMemcpy(elms, h.elms_ptr(), ne * elm_size(h.elm_dtype), cudaMemcpyHostToDevice));
   }
-  return ISPM_OK;
+  return attach_stage_records(h);
 }
 
 int DeviceSlell::upload_f16(const HostSlell &h)
@@ -136,7 +273,7 @@ int DeviceSlell::upload_f16(const HostSlell &h)
     ISPM_CUDA_TRY(cudaMemcpy(cols, h.cols.data(), nc * 4, cudaMemcpyHostToDevice));
   if (ne)
     ISPM_CUDA_TRY(cudaMemcpy(elms, b.data(), ne * 2, cudaMemcpyHostToDevice));
-  return ISPM_OK;
+  return attach_stage_records(h);
 }
 
 int DeviceSlell::update_elms(const HostSlell &h)
@@ -415,6 +552,37 @@ int ispm_dslell_upload(const ispm_slell *h, ispm_dslell **out)
     return st;
   }
   *out = d;
+  return ISPM_OK;
+}
+
+int ispm_dslell_upload_f16(const ispm_slell *h, ispm_dslell **out)
+{
+  clear_error();
+  if (!h || !out)
+    return fail(ISPM_ERR_INVALID, "NULL argument");
+  *out = nullptr;
+  ispm_dslell *d = new (std::nothrow) ispm_dslell;
+  if (!d)
+    return fail(ISPM_ERR_NOMEM, "host allocation");
+  int st = d->d.upload_f16(h->m);
+  if (st) {
+    delete d;
+    return st;
+  }
+  *out = d;
+  return ISPM_OK;
+}
+
+int ispm_slell_stage_records(const ispm_slell *m, int *out, long long cap, long long *n_ints)
+{
+  clear_error();
+  if (!m || !n_ints || (cap > 0 && !out))
+    return fail(ISPM_ERR_INVALID, "NULL argument");
+  std::vector<int> rec;
+  stage_records(m->m, rec);
+  *n_ints = (long long)rec.size();
+  for (long long k = 0; k < cap && k < (long long)rec.size(); k++)
+    out[k] = rec[(size_t)k];
   return ISPM_OK;
 }
 

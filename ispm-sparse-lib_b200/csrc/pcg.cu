@@ -1147,7 +1147,12 @@ int ispm_solver_create(int n, const int *row_ptr, const int *cols, const double 
     } else if (int e = S.Ain.upload(S.inner, S.inner, n, row_ptr, cols, vals)) {
       return e;
     }
-    if (int e = S.A64.upload(ISPM_F64, ISPM_F64, n, row_ptr, cols, vals, &S.Ain.fmt))
+    // the FP64 operator of the reliable updates takes the inner matrix's
+    // shape, unless the inner matrix is an FP16 split (its shape was chosen
+    // for the off-diagonal part alone): then A64 gets its own min-bytes shape
+    const bool split = S.inner == ISPM_F32 && S.opts.matrix_f16;
+    if (int e = S.A64.upload(ISPM_F64, ISPM_F64, n, row_ptr, cols, vals,
+                             split ? nullptr : &S.Ain.fmt))
       return e;
     if (S.opts.prec == ISPM_PREC_FSAI_GPU) {
       if (int e = build_fsai_on_device(S, n, row_ptr, cols, vals))

@@ -434,276 +434,8 @@ __global__ void __launch_bounds__(1024, 2) slell_spmv_lanes_kernel(SpmvArgs<T, E
   spmv_body<T, E, H, W, false, DIAG, true>(a);
 }
 
-// ---- staged diagonal walk: the launch shape N = S, H = 1 ------------------
-//
-// One thread per row, a CTA per tile of max(256, S) consecutive rows
-// (fixed slice height, diagonal blocks).  In the reference walk
-// (kernel.h:80-92) the thread of local row r reads x[diag_pos + r - S] for
-// every diagonal of its slice.  When every slice of the tile carries the same
-// diagonal offsets (diag_pos minus the slice's first row), the tile's x
-// windows are the intervals [w_k, w_k + rows) of slice 0's window starts w_k;
-// runs of nearby windows are merged into bands, the bands are copied into
-// shared memory once per CTA (16-byte vector loads, zero outside x), and the
-// walk becomes one streaming element load, one shared-memory load and one FMA
-// per entry: the per-diagonal address arithmetic, the window realignment and
-// the bounds tests of the register walk all drop out.  The first diagonals'
-// elements are requested before the bands are staged (and before the
-// programmatic-launch wait: the matrix does not depend on the predecessor),
-// so the element stream starts at once.  Tiles whose slices differ (grid
-// boundaries) or whose bands exceed the staging budget walk x through the
-// read-only path with bounds tests, as the register walk does.
-constexpr unsigned kStageMinRows = 256;    // rows (threads) of a CTA, at least
-constexpr unsigned kStageMaxDiag = 64;     // diagonals per slice the staged walk handles
-constexpr unsigned kStageWordsPerRow = 12; // x staging budget, words of T per tile row
-constexpr int kStageGap = 32;              // windows this close (in words) share a band
+#include "spmv_staged.cuh"
 
-template <class T, class E>
-__global__ void __launch_bounds__(512, sizeof(T) == 8 ? 3 : 4)
-    slell_spmv_staged_kernel(SpmvArgs<T, E> a)
-{
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *xs = reinterpret_cast<T *>(smem_raw);
-  __shared__ __align__(16) int s_sx[kStageMaxDiag];  // smem start of each diagonal's window
-  __shared__ int s_lo[kStageMaxDiag], s_hi[kStageMaxDiag], s_off[kStageMaxDiag];
-  __shared__ int s_nb, s_total;
-  constexpr int VW = 16 / (int)sizeof(T);  // values of T per 16-byte chunk
-  // element loads issued before the staging (fewer for FP64 vectors: their
-  // registers run out first)
-  constexpr int kStagePre = sizeof(T) == 8 ? 2 : 4;
-
-  const unsigned S = a.slice_height;
-  const unsigned rows = blockDim.x;
-  const unsigned tid = threadIdx.x;
-  const unsigned spb = rows / S;
-  const unsigned b0 = blockIdx.x * spb;
-  const unsigned nsl = min(spb, a.n_slices - b0);
-  const unsigned s = tid / S, r = tid & (S - 1);
-  const bool active = s < nsl;
-  const unsigned b = active ? b0 + s : b0;
-
-  // slice records [elms_end, cols_end, diag_ptr] (conversion.h:393-402)
-  const unsigned *rec = a.sp + 3 * (size_t)b;
-  const unsigned e0 = __ldg(rec), c0 = __ldg(rec + 1), d0 = __ldg(rec + 2);
-  const unsigned e1 = __ldg(rec + 3), c1 = __ldg(rec + 4);
-  const unsigned ed = e0 + (c1 - c0);                 // first diagonal element
-  const unsigned nd = active ? (e1 - ed) / S : 0u;    // diagonals of this slice
-  const unsigned nell = active ? (c1 - c0) / S : 0u;  // explicit-column entries per row
-
-  // element prefetch (matrix data is final before the predecessor ends)
-  const E *__restrict__ ep = a.elms + ed + r;
-  E pre[kStagePre];
-#pragma unroll
-  for (int u = 0; u < kStagePre; u++)
-    pre[u] = (unsigned)u < nd ? ld_stream<1>(ep + (size_t)u * S).v[0] : E(0.0f);
-
-  pdl_wait();
-  if (a.skip && *a.skip)
-    return;
-
-  // do all slices of the tile carry slice 0's diagonal offsets?
-  const unsigned *rec0 = a.sp + 3 * (size_t)b0;
-  const unsigned ed0 = __ldg(rec0) + (__ldg(rec0 + 4) - __ldg(rec0 + 1));
-  const unsigned nd0 = (__ldg(rec0 + 3) - ed0) / S;
-  const unsigned dd0 = __ldg(rec0 + 2);
-  bool ok = nd0 <= kStageMaxDiag && nd0 > 0;
-  if (active && r == 0 && nd != nd0)
-    ok = false;
-  if (ok) {
-    for (unsigned idx = tid; idx < nsl * nd0; idx += rows) {
-      const unsigned ss = idx / nd0, k = idx - ss * nd0;
-      const unsigned dss = __ldg(a.sp + 3 * (size_t)(b0 + ss) + 2);
-      if (__ldg(a.sp + dss + k) - ss * S != __ldg(a.sp + dd0 + k))
-        ok = false;
-    }
-  }
-  const bool uniform = __syncthreads_and(ok) != 0;
-
-  bool staged = false;
-  if (uniform) {
-    // bands: runs of ascending window starts less than rows + gap apart
-    if (tid < 32) {
-      const unsigned lane = tid;
-      int nb = 0;
-      for (unsigned base = 0; base < nd0; base += 32) {
-        const unsigned k = base + lane;
-        const bool valid = k < nd0;
-        const int w = valid ? (int)__ldg(a.sp + dd0 + k) - (int)S : 0;
-        const int wp = (valid && k > 0) ? (int)__ldg(a.sp + dd0 + k - 1) - (int)S : 0;
-        const int wn = (k + 1 < nd0) ? (int)__ldg(a.sp + dd0 + k + 1) - (int)S : 0;
-        const bool brk = valid && (k == 0 || w < wp || w - wp > (int)rows + kStageGap);
-        const bool nbrk = k + 1 < nd0 && (wn < w || wn - w > (int)rows + kStageGap);
-        const unsigned m = __ballot_sync(0xffffffffu, brk);
-        const int bid = nb + __popc(m & (0xffffffffu >> (31 - lane))) - 1;
-        if (brk)
-          s_lo[bid] = w;
-        if (valid && (k + 1 == nd0 || nbrk))
-          s_hi[bid] = w + (int)rows;
-        if (valid)
-          s_sx[k] = bid;  // band of diagonal k, replaced by its window start below
-        nb += __popc(m);
-      }
-      __syncwarp();
-      if (lane == 0) {
-        // shared-memory placement: word c of x sits at a position congruent
-        // to c modulo VW, so 16-byte chunks of x land on 16-byte chunks
-        int off = 0;
-        for (int q = 0; q < nb; q++) {
-          const int al = ((s_lo[q] % VW) + VW) % VW;
-          off = (off + VW - 1) / VW * VW + al;
-          s_off[q] = off;
-          off += s_hi[q] - s_lo[q];
-        }
-        s_nb = nb;
-        s_total = (off + VW - 1) / VW * VW;
-      }
-      __syncwarp();
-      for (unsigned k = lane; k < nd0; k += 32) {
-        const int q = s_sx[k];
-        s_sx[k] = s_off[q] + ((int)__ldg(a.sp + dd0 + k) - (int)S - s_lo[q]);
-      }
-    }
-    __syncthreads();
-    staged = s_total <= a.stage_words;
-    if (staged) {
-      const int n = (int)a.n_cols;
-      const int nb = s_nb;
-      for (int q = 0; q < nb; q++) {
-        const int lo = s_lo[q], hi = s_hi[q];
-        const int c0q = lo >= 0 ? lo / VW * VW : -((-lo + VW - 1) / VW) * VW;
-        const int nch = (hi - c0q + VW - 1) / VW;
-        T *dst = xs + (s_off[q] - (lo - c0q));
-        for (int c = (int)tid; c < nch; c += (int)rows) {
-          const int col = c0q + c * VW;
-          T v[VW];
-          if (a.x_al16 && col >= 0 && col + VW <= n) {
-            if constexpr (sizeof(T) == 4) {
-              const float4 f = __ldg(reinterpret_cast<const float4 *>(a.x + col));
-              v[0] = f.x;
-              v[1] = f.y;
-              v[2] = f.z;
-              v[3] = f.w;
-            } else {
-              const double2 f = __ldg(reinterpret_cast<const double2 *>(a.x + col));
-              v[0] = f.x;
-              v[1] = f.y;
-            }
-          } else {
-#pragma unroll
-            for (int u = 0; u < VW; u++) {
-              const int cc = col + u;
-              v[u] = (cc >= 0 && cc < n) ? __ldg(a.x + cc) : T(0);
-            }
-          }
-          if constexpr (sizeof(T) == 4)
-            *reinterpret_cast<float4 *>(dst + c * VW) = make_float4(v[0], v[1], v[2], v[3]);
-          else
-            *reinterpret_cast<double2 *>(dst + c * VW) = make_double2(v[0], v[1]);
-        }
-      }
-      __syncthreads();
-    }
-  }
-
-  T acc = T(0);
-  if (staged) {
-    const T *xt = xs + tid;
-#pragma unroll
-    for (int u = 0; u < kStagePre; u++)
-      if ((unsigned)u < nd)
-        acc = fma(T(pre[u]), xt[s_sx[u]], acc);
-    unsigned k = kStagePre;
-    for (; k < 4 && k < nd; k++)  // from here on s_sx + k is 16-byte aligned
-      acc = fma(T(ld_stream<1>(ep + (size_t)k * S).v[0]), xt[s_sx[k]], acc);
-    for (; k + 8 <= nd; k += 8) {
-      E e[8];
-#pragma unroll
-      for (int u = 0; u < 8; u++)
-        e[u] = ld_stream<1>(ep + (size_t)(k + u) * S).v[0];
-      const int4 q0 = *reinterpret_cast<const int4 *>(s_sx + k);
-      const int4 q1 = *reinterpret_cast<const int4 *>(s_sx + k + 4);
-      acc = fma(T(e[0]), xt[q0.x], acc);
-      acc = fma(T(e[1]), xt[q0.y], acc);
-      acc = fma(T(e[2]), xt[q0.z], acc);
-      acc = fma(T(e[3]), xt[q0.w], acc);
-      acc = fma(T(e[4]), xt[q1.x], acc);
-      acc = fma(T(e[5]), xt[q1.y], acc);
-      acc = fma(T(e[6]), xt[q1.z], acc);
-      acc = fma(T(e[7]), xt[q1.w], acc);
-    }
-    for (; k < nd; k++)
-      acc = fma(T(ld_stream<1>(ep + (size_t)k * S).v[0]), xt[s_sx[k]], acc);
-  } else if (active) {
-    // read-only-path walk of this thread's own slice (kernel.h:80-92)
-    const unsigned adj = r - S;
-#pragma unroll
-    for (int u = 0; u < kStagePre; u++)
-      if ((unsigned)u < nd)
-        acc = fma(T(pre[u]), ld_x_guard(a.x, __ldg(a.sp + d0 + u) + adj, a.n_cols), acc);
-#pragma unroll 4
-    for (unsigned k = kStagePre; k < nd; k++)
-      acc = fma(T(ld_stream<1>(ep + (size_t)k * S).v[0]),
-                ld_x_guard(a.x, __ldg(a.sp + d0 + k) + adj, a.n_cols), acc);
-  }
-  // entries off the slice's diagonals, with explicit columns (kernel.h:70-79)
-#pragma unroll 2
-  for (unsigned j = 0; j < nell; j++) {
-    const size_t q = (size_t)j * S + r;
-    acc = fma(T(ld_stream<1>(a.elms + e0 + q).v[0]),
-              ld_x_guard(a.x, ld_stream<1>(a.cols + c0 + q).v[0], a.n_cols), acc);
-  }
-
-  pdl_trigger();
-  const unsigned row = b0 * S + tid;
-  if constexpr (std::is_same<E, __half>::value) {
-    if (active)
-      acc = a.dg ? fma(__ldcs(a.dg + row), ld_x_guard(a.x, row, a.n_cols), acc * a.inv_scale)
-                 : acc * a.inv_scale;
-  }
-  if (active)
-    a.y[row] = acc;
-  if (a.ep.out) {
-    double dv = 0.0, dw = 0.0;
-    const bool two = a.ep.out2 != nullptr;
-    if (active) {
-      const double vv = (double)static_cast<const T *>(a.ep.v)[row];
-      dv = (double)acc * vv;
-      if (two)
-        dw = vv * vv;
-    }
-    if (two)
-      finish_dot2(dv, dw, a.ep);
-    else
-      finish_dot(dv, a.ep);
-  }
-}
-
-// The staged walk serves this launch: diagonal blocks, fixed slice height
-// in [16, 512], one row per thread and S threads per slice.
-bool staged_shape(const ispm_launch_params &p, const ispm_slell_view &m)
-{
-  return m.diags && !m.var_height && m.hblock == 1 && p.H == 1 && p.N == m.slice_height &&
-         m.slice_height >= 16 && m.slice_height <= 512;
-}
-
-template <class T, class E>
-int launch_staged(SpmvArgs<T, E> args, cudaStream_t stream)
-{
-  const unsigned rows = args.slice_height > kStageMinRows ? args.slice_height : kStageMinRows;
-  const unsigned spb = rows / args.slice_height;
-  const unsigned grid = (args.n_slices + spb - 1) / spb;
-  // staging buffer: kStageWordsPerRow values per row, at most 40 KB so that
-  // with the kernel's static tables it stays inside the 48 KB a launch gets
-  // without opting in to more
-  const size_t smem = std::min<size_t>((size_t)kStageWordsPerRow * rows * sizeof(T), 40960);
-  args.stage_words = (int)(smem / sizeof(T));
-  cudaError_t e = launch_kernel(slell_spmv_staged_kernel<T, E>, dim3(grid), dim3(rows), smem,
-                                stream, args.pdl != 0, args);
-  if (e == cudaSuccess)
-    e = cudaPeekAtLastError();
-  if (e != cudaSuccess)
-    return fail(ISPM_ERR_CUDA, "SpMV launch: %s", cudaGetErrorString(e));
-  return ISPM_OK;
-}
 
 template <class T, class E, int H, int W, bool VAR, bool DIAG, bool LANES = false>
 int launch_one(const SpmvArgs<T, E> &args, unsigned tps, cudaStream_t stream)
@@ -808,8 +540,9 @@ int launch_te(const ispm_launch_params &p, const ispm_slell_view &m, const void 
   if (!aligned(m.elms, p.H * sizeof(E)) || !aligned(m.cols, p.H * sizeof(unsigned)) ||
       !aligned(y, p.H * sizeof(T)))
     return fail(ISPM_ERR_INVALID, "matrix arrays or y not aligned to H=%u elements", p.H);
-  if (!ln && staged_shape(p, m))
-    return launch_staged<T, E>(a, s);
+  StageInfo si;
+  if (!ln && staged_shape(p, m, si))
+    return launch_staged<T, E>(a, si, s);
   switch (p.H) {
   case 1: return launch_h<T, E, 1>(a, m, p.N, s, ln != nullptr);
   case 2: return launch_h<T, E, 2>(a, m, p.N, s, ln != nullptr);

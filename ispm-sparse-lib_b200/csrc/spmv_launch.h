@@ -63,6 +63,15 @@ struct SpmvSplit {
   float inv_scale = 1.f;
 };
 
+// Tile records of the device matrix whose slice_ptr array is `slice_ptr`
+// (registered by DeviceSlell uploads, dropped on release) and the largest
+// staged-band footprint (shared-memory words) over its tiles.
+struct StageInfo {
+  const int *rec = nullptr;
+  int max_words = 0;
+};
+bool find_stage_records(const unsigned *slice_ptr, unsigned n_slices, StageInfo &out);
+
 // Validate and launch y = A x on `s`.  `skip` (device int, may be NULL): the
 // kernel returns at once when it holds a nonzero value.
 // pdl: launch as a programmatic dependent of the stream's previous kernel
@@ -80,11 +89,38 @@ unsigned spmv_grid(const ispm_launch_params &p, const ispm_slell_view &m);
 unsigned spmv_cta_rows(const ispm_launch_params &p, const ispm_slell_view &m);
 
 // Device-resident sliced-ELL matrix.
+// Staged diagonal walk (launch shape N = S, H = 1): the matrix is cut into
+// tiles of kStageTileRows rows; every tile has a record of kStageRecInts
+// ints, computed on the host from the slice records when a diagonal-block
+// matrix of fixed slice height is uploaded:
+//   [0] 1 when every slice of the tile carries slice 0's diagonal offsets
+//       (diag_pos minus the slice's first row) and there are 1..64 of them;
+//   [1] nb, the number of x bands (runs of nearby windows, at most 8);
+//   [2] shared-memory words the bands take (16-byte chunk aligned);
+//   [3] nd, the diagonals of every slice of the tile;
+//   [4 + 3q .. 6 + 3q] band q: first x column, end column, shared-memory
+//       start (congruent to the first column modulo 4);
+//   [28 + k] shared-memory word of x[w_k], w_k = the window start of
+//       diagonal k for the tile's first row (x[w_k + t] serves tile row t).
+constexpr unsigned kStageTileRows = 1024;
+constexpr int kStageRecInts = 96;
+constexpr int kStageMaxBands = 8;
+constexpr int kStageMaxDiag = 64;
+constexpr int kStageGap = 32;  // windows this close (in words) share a band
+
+// Tile records of h (empty unless h is diagonal-block, fixed height, and its
+// slice height divides kStageTileRows).
+void stage_records(const HostSlell &h, std::vector<int> &rec);
+
 struct DeviceSlell {
   ispm_slell_view meta{};  // host copy of the metadata; pointers are device pointers
   unsigned *slice_ptr = nullptr;
   unsigned *cols = nullptr;
   void *elms = nullptr;
+  int *stage_rec = nullptr;  // tile records of the staged walk (device), or NULL
+  int stage_max_words = 0;
+  // build, upload and register the tile records of h (no-op for other shapes)
+  int attach_stage_records(const HostSlell &h);
   ispm_slell_view view() const
   {
     ispm_slell_view v = meta;

@@ -110,6 +110,8 @@ def _declare(L):
         "ispm_slell_spmv_bytes": (C.c_ulonglong, [vp, i, i]),
         "ispm_slell_free": (None, [vp]),
         "ispm_dslell_upload": (i, [vp, C.POINTER(vp)]),
+        "ispm_dslell_upload_f16": (i, [vp, C.POINTER(vp)]),
+        "ispm_slell_stage_records": (i, [vp, vp, C.c_longlong, C.POINTER(C.c_longlong)]),
         "ispm_dslell_update_elms": (i, [vp, vp]),
         "ispm_dslell_get_view": (i, [vp, C.POINTER(slell_view)]),
         "ispm_dslell_free": (None, [vp]),
@@ -310,6 +312,22 @@ class slell_matrix:
         _check(_lib().ispm_dslell_upload(self._h, C.byref(out)))
         return device_slell_matrix(out.value, owner=True)
 
+    def upload_f16(self) -> "device_slell_matrix":
+        """Device copy with FP16 elements (every FP32 element must be an exact
+        binary16 value, as in an FP16 split)."""
+        out = C.c_void_p()
+        _check(_lib().ispm_dslell_upload_f16(self._h, C.byref(out)))
+        return device_slell_matrix(out.value, owner=True)
+
+    def stage_records(self) -> np.ndarray:
+        """Tile records of the staged SpMV walk (96 ints per 1024-row tile)."""
+        L = _lib()
+        n = C.c_longlong()
+        _check(L.ispm_slell_stage_records(self._h, None, 0, C.byref(n)))
+        out = np.zeros(max(n.value, 1), np.int32)
+        _check(L.ispm_slell_stage_records(self._h, _ptr(out), n.value, C.byref(n)))
+        return out[: n.value].reshape(-1, 96) if n.value else out[:0].reshape(0, 96)
+
 
 class device_slell_matrix:
     """Device sliced-ELL matrix (slell_matrix<E, device_memory_space_tag>)."""
@@ -420,26 +438,14 @@ class device_split_f16:
         Ao = csr_matrix(n, n, orp, np.ascontiguousarray(A.cols[keep], np.int32), vals)
         self.host = csr_to_slell_guess_format(Ao) if fmt is None else csr_to_slell(Ao, *fmt)
         v = self.host.view()
-        el = self.host.elms.astype(np.float16)
-        if not np.array_equal(el.astype(np.float32), self.host.elms):
-            raise IspmError(ERR_INVALID, "split values are not binary16 values")
-        dev = torch.device("cuda")
-        self._sp = torch.from_numpy(self.host.slice_ptr.view(np.int32).copy()).to(dev)
-        self._cols = torch.from_numpy(self.host.cols.view(np.int32).copy() if v.n_cols_arr
-                                      else np.zeros(4, np.int32)).to(dev)
-        self._elms = torch.from_numpy(el if el.size else np.zeros(8, np.float16)).to(dev)
+        # the library's FP16 upload (it checks every value is a binary16 value)
+        self.dev = self.host.upload_f16()
         dg = np.zeros(v.n_rows, np.float32)
         dg[:n] = diag
-        self.diag = torch.from_numpy(dg).to(dev)
+        self.diag = torch.from_numpy(dg).to(torch.device("cuda"))
         self.scale = sc
         self.inv_scale = 1.0 / sc
-        dv = slell_view()
-        for f, _ in slell_view._fields_:
-            setattr(dv, f, getattr(v, f))
-        dv.elm_dtype = F16
-        dv.slice_ptr, dv.cols = self._sp.data_ptr(), self._cols.data_ptr()
-        dv.elms = self._elms.data_ptr()
-        self.view_ = dv
+        self.view_ = self.dev.view()
 
     def view(self) -> slell_view:
         return self.view_

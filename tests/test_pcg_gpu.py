@@ -175,24 +175,28 @@ def test_reordering_rejects_a_given_pair(ispm, cuda, gen):
     ispm.PCGSolver(A, G1, G2, reorder="auto")  # automatic mode leaves it alone
 
 
-@pytest.mark.parametrize("inner", [np.float32, np.float64])
-def test_solver_edge_cases(ispm, oracle, cuda, gen, inner):
+@pytest.mark.parametrize("inner,f16", [(np.float32, False), (np.float64, False),
+                                       (np.float32, True)], ids=["f32", "f64", "f32-split"])
+def test_solver_edge_cases(ispm, oracle, cuda, gen, inner, f16):
     """Zero right-hand side (x = 0 at once), a 1 x 1 system and a system the
-    starting guess already solves exactly."""
+    starting guess already solves exactly; also with A's inner copy stored as
+    the FP16 split (f32-split), where the 1 x 1 and diagonal systems have an
+    empty off-diagonal part (zero-size conversion, diagonal-only epilogue)."""
+    kw = dict(matrix_f16=f16)
     A = gen.poisson7(5)
-    S = ispm.PCGSolver(A, inner=inner, tol=1e-10, prec="fsai_gpu")
+    S = ispm.PCGSolver(A, inner=inner, tol=1e-10, prec="fsai_gpu", **kw)
     x, st = S.solve_host(np.zeros(A.n_rows))
     assert st["converged"] and st["iterations"] == 0 and not np.any(x)
     one = ispm.csr_matrix(1, 1, np.array([0, 1], np.int32), np.array([0], np.int32),
                           np.array([4.0]))
-    S1 = ispm.PCGSolver(one, inner=inner, tol=1e-10, prec="fsai_gpu")
+    S1 = ispm.PCGSolver(one, inner=inner, tol=1e-10, prec="fsai_gpu", **kw)
     x1, st1 = S1.solve_host(np.array([2.0]))
     assert st1["converged"] and abs(x1[0] - 0.5) <= 1e-12
     # a diagonal system: one iteration
     n = 1000
     d = np.arange(1, n + 1, dtype=np.float64)
     D = ispm.csr_matrix(n, n, np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32), d)
-    SD = ispm.PCGSolver(D, inner=inner, tol=1e-10, prec="fsai_gpu")
+    SD = ispm.PCGSolver(D, inner=inner, tol=1e-10, prec="fsai_gpu", **kw)
     xd, std = SD.solve_host(d.copy())
     assert std["converged"] and std["iterations"] <= 2
     assert np.allclose(xd, 1.0, rtol=0, atol=1e-9)
