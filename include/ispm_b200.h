@@ -131,7 +131,7 @@ int ispm_dslell_upload(const ispm_slell *h, ispm_dslell **out);
 int ispm_dslell_upload_f16(const ispm_slell *h, ispm_dslell **out);
 /* Diagnostics of the staged SpMV walk (launch shape N = S, H = 1; no
  * counterpart in the reference): the tile records an upload of m computes
- * (96 ints per 1024-row tile; none unless m has diagonal blocks and a fixed
+ * (224 ints per 1024-row tile; none unless m has diagonal blocks and a fixed
  * slice height dividing 1024).  *n_ints receives the count; at most cap ints
  * are written to out (which may be NULL with cap 0). */
 int ispm_slell_stage_records(const ispm_slell *m, int *out, long long cap, long long *n_ints);

@@ -50,52 +50,55 @@ void stage_records(const HostSlell &h, std::vector<int> &rec)
 {
   rec.clear();
   const unsigned S = h.slice_height;
-  if (!h.diags || h.var_height || h.hblock != 1 || !S || kStageTileRows % S || !h.n_slices)
+  if (!h.diags || h.var_height || h.hblock != 1 || S < 16 || kStageTileRows % S || !h.n_slices)
     return;
-  const unsigned spt = kStageTileRows / S;
+  const unsigned spt = kStageTileRows / S;  // <= 64 slices per tile
   const unsigned n_tiles = (h.n_slices + spt - 1) / spt;
   rec.assign((size_t)n_tiles * kStageRecInts, 0);
   const unsigned *sp = h.slice_ptr.data();
-  // slice b: [elms_end, cols_end, diag_ptr] at 3b (conversion.h:393-402)
-  auto n_diag = [&](unsigned b) {
-    const unsigned e0 = sp[3 * b], c0 = sp[3 * b + 1], e1 = sp[3 * b + 3], c1 = sp[3 * b + 4];
-    return (int)((e1 - e0 - (c1 - c0)) / S);
-  };
   const long long rows = kStageTileRows;
+  std::vector<long long> win, all;
   for (unsigned t = 0; t < n_tiles; t++) {
     int *r = rec.data() + (size_t)t * kStageRecInts;
     const unsigned b0 = t * spt, nsl = std::min(spt, h.n_slices - b0);
-    const int nd0 = n_diag(b0);
-    const unsigned dd0 = sp[3 * b0 + 2];
-    bool uniform = nd0 >= 1 && nd0 <= kStageMaxDiag;
-    for (unsigned s = 1; s < nsl && uniform; s++) {
-      const unsigned b = b0 + s, dd = sp[3 * b + 2];
-      if (n_diag(b) != nd0) {
-        uniform = false;
-        break;
+    // window starts of every slice's diagonals (slice b: [elms_end, cols_end,
+    // diag_ptr] at 3b, conversion.h:393-402), relative to the tile's first row
+    all.clear();
+    bool ascending = true;
+    for (unsigned s = 0; s < nsl; s++) {
+      const unsigned b = b0 + s;
+      const unsigned e0 = sp[3 * b], c0 = sp[3 * b + 1], e1 = sp[3 * b + 3], c1 = sp[3 * b + 4];
+      const unsigned nd = (e1 - e0 - (c1 - c0)) / S, dd = sp[3 * b + 2];
+      for (unsigned k = 0; k < nd; k++) {
+        const long long w = (long long)sp[dd + k] - S - (long long)s * S;
+        if (k && w <= all.back())
+          ascending = false;
+        all.push_back(w);
       }
-      for (int k = 0; k < nd0 && uniform; k++)
-        uniform = sp[dd + k] - s * S == sp[dd0 + k];
     }
-    if (!uniform)
+    win = all;
+    std::sort(win.begin(), win.end());
+    win.erase(std::unique(win.begin(), win.end()), win.end());
+    const int nu = (int)win.size();
+    if (!ascending || nu < 1 || nu > kStageMaxDiag)
       continue;  // r[0] = 0: the tile reads x directly
-    // runs of ascending window starts less than rows + gap apart share a band
+    // absolute window starts; runs less than rows + gap apart share a band
+    const long long row0 = (long long)b0 * S;
     long long lo[kStageMaxDiag], hi[kStageMaxDiag];
     int band[kStageMaxDiag], nb = 0;
-    for (int k = 0; k < nd0; k++) {
-      const long long w = (long long)sp[dd0 + k] - S;
-      const long long wp = k ? (long long)sp[dd0 + k - 1] - S : 0;
-      if (k == 0 || w < wp || w - wp > rows + kStageGap) {
+    for (int u = 0; u < nu; u++) {
+      const long long w = row0 + win[u];
+      if (u == 0 || w - (row0 + win[u - 1]) > rows + kStageGap) {
         lo[nb] = w;
         nb++;
       }
       hi[nb - 1] = w + rows;
-      band[k] = nb - 1;
+      band[u] = nb - 1;
     }
-    if (nb > kStageMaxBands)
+    if (nb > kStageMaxBands || lo[0] < INT32_MIN / 2 || hi[nb - 1] > INT32_MAX / 2)
       continue;
     // shared-memory placement: column c sits at a word congruent to c
-    // modulo 4, so 16-byte chunks of x (FP32 or FP64) land on 16-byte chunks
+    // modulo 4, so 16-byte chunks of x land on 16-byte chunks
     long long off = 0, offs[kStageMaxBands];
     for (int q = 0; q < nb; q++) {
       off = (off + 3) / 4 * 4 + (((lo[q] % 4) + 4) % 4);
@@ -103,23 +106,45 @@ void stage_records(const HostSlell &h, std::vector<int> &rec)
       off += hi[q] - lo[q];
     }
     const long long total = (off + 3) / 4 * 4;
-    if (total > (1 << 20) || lo[0] < INT32_MIN / 2 || hi[nb - 1] > INT32_MAX / 2)
+    if (total >= (1 << 24))
       continue;
     r[0] = 1;
     r[1] = nb;
     r[2] = (int)total;
-    r[3] = nd0;
+    r[3] = nu;
     for (int q = 0; q < nb; q++) {
       r[4 + 3 * q] = (int)lo[q];
       r[5 + 3 * q] = (int)hi[q];
       r[6 + 3 * q] = (int)offs[q];
     }
-    for (int k = 0; k < nd0; k++) {
-      const int q = band[k];
-      r[28 + k] = (int)(offs[q] + ((long long)sp[dd0 + k] - S - lo[q]));
+    // entries grouped by the shared-memory start modulo 4
+    int i = 0;
+    for (int m = 0; m < 4; m++) {
+      for (int u = 0; u < nu; u++) {
+        const int q = band[u];
+        const long long sx = offs[q] + (row0 + win[u] - lo[q]);
+        if ((sx & 3) == m)
+          r[32 + i++] = (int)sx | (u << 24);
+      }
+      r[28 + m] = i;
+    }
+    // slice masks over the window starts
+    for (unsigned s = 0; s < nsl; s++) {
+      const unsigned b = b0 + s;
+      const unsigned e0 = sp[3 * b], c0 = sp[3 * b + 1], e1 = sp[3 * b + 3], c1 = sp[3 * b + 4];
+      const unsigned nd = (e1 - e0 - (c1 - c0)) / S, dd = sp[3 * b + 2];
+      unsigned long long mask = 0;
+      for (unsigned k = 0; k < nd; k++) {
+        const long long w = (long long)sp[dd + k] - S - (long long)s * S;
+        const int u = (int)(std::lower_bound(win.begin(), win.end(), w) - win.begin());
+        mask |= 1ull << u;
+      }
+      r[96 + 2 * s] = (int)(unsigned)(mask & 0xffffffffull);
+      r[97 + 2 * s] = (int)(unsigned)(mask >> 32);
     }
   }
 }
+
 
 namespace {
 struct StageEntry {

@@ -540,9 +540,11 @@ int launch_te(const ispm_launch_params &p, const ispm_slell_view &m, const void 
   if (!aligned(m.elms, p.H * sizeof(E)) || !aligned(m.cols, p.H * sizeof(unsigned)) ||
       !aligned(y, p.H * sizeof(T)))
     return fail(ISPM_ERR_INVALID, "matrix arrays or y not aligned to H=%u elements", p.H);
-  StageInfo si;
-  if (!ln && staged_shape(p, m, si))
-    return launch_staged<T, E>(a, si, s);
+  if constexpr (std::is_same<T, float>::value) {
+    StageInfo si;
+    if (!ln && staged_shape(ISPM_F32, p, m, y, si))
+      return launch_staged<E>(a, si, s);
+  }
   switch (p.H) {
   case 1: return launch_h<T, E, 1>(a, m, p.N, s, ln != nullptr);
   case 2: return launch_h<T, E, 2>(a, m, p.N, s, ln != nullptr);

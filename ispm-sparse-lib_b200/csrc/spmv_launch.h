@@ -89,21 +89,28 @@ unsigned spmv_grid(const ispm_launch_params &p, const ispm_slell_view &m);
 unsigned spmv_cta_rows(const ispm_launch_params &p, const ispm_slell_view &m);
 
 // Device-resident sliced-ELL matrix.
-// Staged diagonal walk (launch shape N = S, H = 1): the matrix is cut into
-// tiles of kStageTileRows rows; every tile has a record of kStageRecInts
-// ints, computed on the host from the slice records when a diagonal-block
-// matrix of fixed slice height is uploaded:
-//   [0] 1 when every slice of the tile carries slice 0's diagonal offsets
-//       (diag_pos minus the slice's first row) and there are 1..64 of them;
-//   [1] nb, the number of x bands (runs of nearby windows, at most 8);
+// Staged diagonal walk (FP32 vectors, launch shape N = S, H = 1): the matrix
+// is cut into tiles of kStageTileRows rows; every tile has a record of
+// kStageRecInts ints, computed on the host from the slice records when a
+// diagonal-block matrix of fixed slice height is uploaded.  A diagonal of
+// slice s at diag_pos d serves tile row t = s S + r from x[w + t] with the
+// window start w = d - S - s S; the tile's windows are the union W of those
+// starts over its slices (ascending, u = 0 .. nu - 1):
+//   [0] 1 when the tile is staged: 1..64 window starts, every slice's own
+//       diagonals in ascending order, at most 8 bands;
+//   [1] nb, the number of x bands (runs of nearby windows);
 //   [2] shared-memory words the bands take (16-byte chunk aligned);
-//   [3] nd, the diagonals of every slice of the tile;
+//   [3] nu, the number of window starts;
 //   [4 + 3q .. 6 + 3q] band q: first x column, end column, shared-memory
 //       start (congruent to the first column modulo 4);
-//   [28 + k] shared-memory word of x[w_k], w_k = the window start of
-//       diagonal k for the tile's first row (x[w_k + t] serves tile row t).
+//   [28 + m] end of group m (m = 0..3) in the entry list: the windows whose
+//       shared-memory start is congruent to m modulo 4;
+//   [32 + i] entry i: shared-memory word of x[w_u] | u << 24, grouped by m;
+//   [96 + 2s], [97 + 2s] slice s of the tile: bit u of this 64-bit mask is
+//       set when the slice has a diagonal at window u (its k-th diagonal is
+//       its k-th set bit).
 constexpr unsigned kStageTileRows = 1024;
-constexpr int kStageRecInts = 96;
+constexpr int kStageRecInts = 224;
 constexpr int kStageMaxBands = 8;
 constexpr int kStageMaxDiag = 64;
 constexpr int kStageGap = 32;  // windows this close (in words) share a band

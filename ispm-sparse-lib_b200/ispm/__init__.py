@@ -320,13 +320,13 @@ class slell_matrix:
         return device_slell_matrix(out.value, owner=True)
 
     def stage_records(self) -> np.ndarray:
-        """Tile records of the staged SpMV walk (96 ints per 1024-row tile)."""
+        """Tile records of the staged SpMV walk (224 ints per 1024-row tile)."""
         L = _lib()
         n = C.c_longlong()
         _check(L.ispm_slell_stage_records(self._h, None, 0, C.byref(n)))
         out = np.zeros(max(n.value, 1), np.int32)
         _check(L.ispm_slell_stage_records(self._h, _ptr(out), n.value, C.byref(n)))
-        return out[: n.value].reshape(-1, 96) if n.value else out[:0].reshape(0, 96)
+        return out[: n.value].reshape(-1, 224) if n.value else out[:0].reshape(0, 224)
 
 
 class device_slell_matrix:

@@ -1,70 +1,96 @@
 """Tile records of the staged SpMV walk (ispm_slell_stage_records), checked
-on the host: for every staged tile, every (diagonal k, tile row t) reads a
-shared-memory word inside the tile's bands that holds x[w_k + t] (zero
-outside x), bands are 16-byte aligned the way the kernel copies them, and
-tiles whose slices carry different diagonals are not staged.  The same
-indexing the kernel does (csrc/spmv_staged.cuh), restated in numpy."""
+on the host against a numpy restatement of the kernel's indexing
+(csrc/spmv_staged.cuh): for every staged tile, every slice's k-th diagonal
+is the k-th set bit of its mask, and every thread's four x values (tile rows
+4 tid .. 4 tid + 3) come from the two shared-memory chunks the kernel reads,
+which hold x[w + t] (zero outside x) and lie inside the copied bands;
+windows are grouped by their shift modulo 4."""
 import numpy as np
 import pytest
 
 TILE = 1024
 
 
-def check_records(B, vw):
+def check_records(B):
     v = B.view()
     S, sp = v.slice_height, B.slice_ptr.astype(np.int64)
     recs = B.stage_records()
     spt = TILE // S
-    assert recs.shape == ((v.n_slices + spt - 1) // spt, 96)
+    assert recs.shape == ((v.n_slices + spt - 1) // spt, 224)
     staged = 0
     for tile, r in enumerate(recs):
-        b0 = tile * spt
-        nsl = min(spt, v.n_slices - b0)
-        nds = [(sp[3 * b + 3] - sp[3 * b] - (sp[3 * b + 4] - sp[3 * b + 1])) // S
-               for b in range(b0, b0 + nsl)]
-        offs = [sp[sp[3 * b + 2]: sp[3 * b + 2] + nds[0]] - (b - b0) * S
-                if nds[b - b0] == nds[0] else None for b in range(b0, b0 + nsl)]
-        uniform = (1 <= nds[0] <= 64 and all(o is not None and np.array_equal(o, offs[0])
-                                             for o in offs))
         if not r[0]:
             continue
-        assert uniform, tile
         staged += 1
-        nb, total, nd0 = r[1], r[2], r[3]
-        assert nd0 == nds[0] and 1 <= nb <= 8 and total % 4 == 0
-        # smem word -> x column, built band by band as the kernel copies
+        b0 = tile * spt
+        nsl = min(spt, v.n_slices - b0)
+        row0 = b0 * S
+        nb, total, nu = r[1], r[2], r[3]
+        assert 1 <= nb <= 8 and total % 4 == 0 and 1 <= nu <= 64
+        # shared-memory word -> absolute x column, band by band as copied
         col_of = np.full(total, np.iinfo(np.int64).min)
         for q in range(nb):
             lo, hi, off = r[4 + 3 * q], r[5 + 3 * q], r[6 + 3 * q]
             assert off % 4 == lo % 4 and hi > lo
-            c0 = (lo // vw) * vw
-            nch = (hi - c0 + vw - 1) // vw
+            c0 = (lo // 4) * 4
+            nch = (hi - c0 + 3) // 4
             dst0 = off - (lo - c0)
-            assert dst0 >= 0 and dst0 % vw == 0 and dst0 + nch * vw <= total
-            col_of[dst0: dst0 + nch * vw] = c0 + np.arange(nch * vw)
-        t = np.arange(nsl * S)
-        for k in range(nd0):
-            w = int(sp[sp[3 * b0 + 2] + k]) - S
-            p = r[28 + k] + t
-            assert p.min() >= 0 and p.max() < total
-            assert np.array_equal(col_of[p], w + t), (tile, k)
+            assert dst0 >= 0 and dst0 % 4 == 0 and dst0 + nch * 4 <= total
+            col_of[dst0: dst0 + nch * 4] = c0 + np.arange(nch * 4)
+        ends = [r[28 + m] for m in range(4)]
+        assert ends == sorted(ends) and ends[3] == nu
+        sx_of = {}
+        for m in range(4):
+            for i in range(ends[m - 1] if m else 0, ends[m]):
+                e = int(r[32 + i])
+                sx, u = e & 0xFFFFFF, e >> 24
+                assert sx % 4 == m and u not in sx_of
+                sx_of[u] = sx
+        assert sorted(sx_of) == list(range(nu))
+        for s in range(nsl):
+            b = b0 + s
+            nd = (sp[3 * b + 3] - sp[3 * b] - (sp[3 * b + 4] - sp[3 * b + 1])) // S
+            mask = (int(r[97 + 2 * s]) & 0xFFFFFFFF) << 32 | (int(r[96 + 2 * s]) & 0xFFFFFFFF)
+            bits = [u for u in range(64) if mask >> u & 1]
+            assert len(bits) == nd
+            tid = (s * S + np.arange(0, S, 4)) // 4  # threads of the slice
+            for k, u in enumerate(bits):
+                w = int(sp[sp[3 * b + 2] + k]) - S - s * S  # window start, tile-relative
+                sx = sx_of[u]
+                q = (sx >> 2) + tid
+                assert q.min() >= 0 and 4 * (q.max() + 2) <= total + 4
+                words = np.concatenate([4 * q[:, None] + np.arange(8)], axis=0)
+                shift = sx % 4
+                need = words[:, shift: shift + 4]
+                t = 4 * tid[:, None] + np.arange(4)
+                assert np.array_equal(col_of[need], row0 + w + t), (tile, s, k)
+                if shift:  # the second chunk the kernel loads lies inside a band
+                    assert np.all(col_of[4 * (q + 1)] != np.iinfo(np.int64).min)
     return staged, len(recs)
 
 
 @pytest.mark.parametrize("S", [16, 32, 64, 128, 256, 512])
 def test_stage_records_stencils(ispm, gen, S):
-    # grids whose x-lines do not align with the slices (24, 20) stage few or
-    # no tiles; a 32^3 grid stages every tile away from its y faces
     for A in (gen.poisson7(24), gen.stencil_grf(20, 27, 4.0, 1.5, 2), gen.poisson7(32)):
-        B = ispm.csr_to_slell(A, S, 1, 0, 1)
-        for vw in (4, 2):
-            staged, n = check_records(B, vw)
-    # slices of one x-line (S <= 32 at 32^3) put the y-face lines, which lack
-    # the -x-line and +x-line diagonals, into every 1024-row tile of a 32^3
-    # grid; at 64^3 half the tiles hold no y-face line
-    B = ispm.csr_to_slell(gen.poisson7(64 if S <= 32 else 32), S, 1, 0, 1)
-    staged, n = check_records(B, 4)
-    assert staged >= n // 2, (staged, n)
+        staged, n = check_records(ispm.csr_to_slell(A, S, 1, 0, 1))
+        # with slice masks every tile of a stencil matrix stages
+        assert staged == n, (staged, n)
+
+
+def test_stage_records_irregular(ispm, gen):
+    import scipy.sparse as sp
+    # a banded random matrix: slices carry different diagonal sets
+    n = 5000
+    rng = np.random.default_rng(3)
+    offs = [-40, -7, -1, 0, 1, 7, 40]
+    M = sp.diags([rng.uniform(-1, 1, n - abs(o)) for o in offs], offs, format="csr")
+    keep = rng.uniform(size=M.nnz) < 0.8
+    M.data[~keep] = 0.0
+    M.eliminate_zeros()
+    M.sort_indices()
+    A = ispm.csr_matrix(n, n, M.indptr.astype(np.int32), M.indices.astype(np.int32), M.data)
+    for S in (32, 64):
+        check_records(ispm.csr_to_slell(A, S, 1, 0, 1))
 
 
 def test_stage_records_only_for_the_staged_formats(ispm, gen):
