@@ -62,7 +62,8 @@ void stage_records(const HostSlell &h, std::vector<int> &rec)
     int *r = rec.data() + (size_t)t * kStageRecInts;
     const unsigned b0 = t * spt, nsl = std::min(spt, h.n_slices - b0);
     // window starts of every slice's diagonals (slice b: [elms_end, cols_end,
-    // diag_ptr] at 3b, conversion.h:393-402), relative to the tile's first row
+    // diag_ptr] at 3b, conversion.h:393-402): the x column that tile row 0
+    // would read, so x[w + t] serves tile row t (diag_pos is absolute)
     all.clear();
     bool ascending = true;
     for (unsigned s = 0; s < nsl; s++) {
@@ -82,13 +83,12 @@ void stage_records(const HostSlell &h, std::vector<int> &rec)
     const int nu = (int)win.size();
     if (!ascending || nu < 1 || nu > kStageMaxDiag)
       continue;  // r[0] = 0: the tile reads x directly
-    // absolute window starts; runs less than rows + gap apart share a band
-    const long long row0 = (long long)b0 * S;
+    // runs of window starts less than rows + gap apart share a band
     long long lo[kStageMaxDiag], hi[kStageMaxDiag];
     int band[kStageMaxDiag], nb = 0;
     for (int u = 0; u < nu; u++) {
-      const long long w = row0 + win[u];
-      if (u == 0 || w - (row0 + win[u - 1]) > rows + kStageGap) {
+      const long long w = win[u];
+      if (u == 0 || w - win[u - 1] > rows + kStageGap) {
         lo[nb] = w;
         nb++;
       }
@@ -122,7 +122,7 @@ void stage_records(const HostSlell &h, std::vector<int> &rec)
     for (int m = 0; m < 4; m++) {
       for (int u = 0; u < nu; u++) {
         const int q = band[u];
-        const long long sx = offs[q] + (row0 + win[u] - lo[q]);
+        const long long sx = offs[q] + (win[u] - lo[q]);
         if ((sx & 3) == m)
           r[32 + i++] = (int)sx | (u << 24);
       }

@@ -24,7 +24,6 @@ def check_records(B):
         staged += 1
         b0 = tile * spt
         nsl = min(spt, v.n_slices - b0)
-        row0 = b0 * S
         nb, total, nu = r[1], r[2], r[3]
         assert 1 <= nb <= 8 and total % 4 == 0 and 1 <= nu <= 64
         # shared-memory word -> absolute x column, band by band as copied
@@ -55,15 +54,16 @@ def check_records(B):
             assert len(bits) == nd
             tid = (s * S + np.arange(0, S, 4)) // 4  # threads of the slice
             for k, u in enumerate(bits):
-                w = int(sp[sp[3 * b + 2] + k]) - S - s * S  # window start, tile-relative
+                dp = int(sp[sp[3 * b + 2] + k])  # diag_pos: local row r reads x[dp + r - S]
                 sx = sx_of[u]
                 q = (sx >> 2) + tid
                 assert q.min() >= 0 and 4 * (q.max() + 2) <= total + 4
                 words = np.concatenate([4 * q[:, None] + np.arange(8)], axis=0)
                 shift = sx % 4
                 need = words[:, shift: shift + 4]
-                t = 4 * tid[:, None] + np.arange(4)
-                assert np.array_equal(col_of[need], row0 + w + t), (tile, s, k)
+                t = 4 * tid[:, None] + np.arange(4)  # tile rows
+                local = t - s * S                     # rows within the slice
+                assert np.array_equal(col_of[need], dp + local - S), (tile, s, k)
                 if shift:  # the second chunk the kernel loads lies inside a band
                     assert np.all(col_of[4 * (q + 1)] != np.iinfo(np.int64).min)
     return staged, len(recs)
