@@ -108,15 +108,25 @@ void stage_records(const HostSlell &h, std::vector<int> &rec)
     const long long total = (off + 3) / 4 * 4;
     if (total >= (1 << 24))
       continue;
-    r[0] = 1;
     r[1] = nb;
     r[2] = (int)total;
     r[3] = nu;
+    long long chunks = 0;
     for (int q = 0; q < nb; q++) {
-      r[4 + 3 * q] = (int)lo[q];
-      r[5 + 3 * q] = (int)hi[q];
-      r[6 + 3 * q] = (int)offs[q];
+      const long long c0 = lo[q] >= 0 ? lo[q] / 4 * 4 : -((-lo[q] + 3) / 4) * 4;
+      chunks += (hi[q] - c0 + 3) / 4;
+      r[4 + 3 * q] = (int)c0;
+      r[5 + 3 * q] = (int)chunks;
+      r[6 + 3 * q] = (int)(offs[q] - (lo[q] - c0));
     }
+    // uniform: every slice has all nu windows (so its k-th diagonal is window k)
+    bool all_slices = true;
+    for (unsigned s = 0; s < nsl && all_slices; s++) {
+      const unsigned b = b0 + s;
+      const unsigned e0 = sp[3 * b], c0 = sp[3 * b + 1], e1 = sp[3 * b + 3], c1 = sp[3 * b + 4];
+      all_slices = (int)((e1 - e0 - (c1 - c0)) / S) == nu;
+    }
+    r[0] = all_slices ? 1 : 2;
     // entries grouped by the shared-memory start modulo 4
     int i = 0;
     for (int m = 0; m < 4; m++) {

@@ -542,7 +542,7 @@ int launch_te(const ispm_launch_params &p, const ispm_slell_view &m, const void 
     return fail(ISPM_ERR_INVALID, "matrix arrays or y not aligned to H=%u elements", p.H);
   if constexpr (std::is_same<T, float>::value) {
     StageInfo si;
-    if (!ln && staged_shape(ISPM_F32, p, m, y, si))
+    if (!ln && (!ep || !ep->out || aligned(ep->v, 16)) && staged_shape(ISPM_F32, p, m, y, si))
       return launch_staged<E>(a, si, s);
   }
   switch (p.H) {

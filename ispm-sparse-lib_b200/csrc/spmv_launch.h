@@ -96,13 +96,17 @@ unsigned spmv_cta_rows(const ispm_launch_params &p, const ispm_slell_view &m);
 // slice s at diag_pos d serves tile row t = s S + r from x[w + t] with the
 // window start w = d - S - s S; the tile's windows are the union W of those
 // starts over its slices (ascending, u = 0 .. nu - 1):
-//   [0] 1 when the tile is staged: 1..64 window starts, every slice's own
-//       diagonals in ascending order, at most 8 bands;
+//   [0] 0: not staged; 1: staged, every slice carries all nu windows, in
+//       order (then u is the slice's diagonal index k); 2: staged, slices
+//       differ (the masks below name each slice's diagonals).  Staged tiles
+//       have 1..64 window starts, every slice's diagonals in ascending
+//       order, at most 8 bands;
 //   [1] nb, the number of x bands (runs of nearby windows);
 //   [2] shared-memory words the bands take (16-byte chunk aligned);
 //   [3] nu, the number of window starts;
-//   [4 + 3q .. 6 + 3q] band q: first x column, end column, shared-memory
-//       start (congruent to the first column modulo 4);
+//   [4 + 3q .. 6 + 3q] band q as the CTA copies it: first x column of its
+//       first 16-byte chunk (a multiple of 4), running total of chunks
+//       through band q, shared-memory word of its first chunk;
 //   [28 + m] end of group m (m = 0..3) in the entry list: the windows whose
 //       shared-memory start is congruent to m modulo 4;
 //   [32 + i] entry i: shared-memory word of x[w_u] | u << 24, grouped by m;

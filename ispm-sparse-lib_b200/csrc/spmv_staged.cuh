@@ -12,13 +12,16 @@
 // shared memory once (16-byte loads, zero outside x).  A thread's four x
 // values then sit in two aligned 16-byte shared-memory chunks, shifted by
 // the window's start modulo 4; the host groups the windows by that shift, so
-// each group's realignment is fixed at compile time.  Slices of a tile may
-// carry different diagonals (grid faces): each slice has a mask over the
-// tile's windows, its k-th diagonal being its k-th set bit.  All of this is
-// computed on the host when the matrix is uploaded (stage_records), so a
-// CTA's set-up is one coalesced load of its record beside its slice header.
-// Tiles with more than 64 windows, more than 8 bands or bands beyond the
-// buffer read x through the read-only path with bounds tests.
+// each group's realignment is fixed at compile time.  In the common tile,
+// every slice carries every window and an entry names the diagonal
+// directly, so the element loads of a group are independent and the
+// compiler batches them; tiles whose slices differ (grid faces) take a mask
+// per slice over the tile's windows (its k-th diagonal is its k-th set
+// bit).  All of this is computed on the host when the matrix is uploaded
+// (stage_records), so a CTA's set-up is one coalesced load of its record
+// beside its slice header.  Tiles with more than 64 windows, more than 8
+// bands or bands beyond the buffer read x through the read-only path with
+// bounds tests.
 
 constexpr int kStageThreads = 256;
 constexpr int kStageMaxChunks = 4;  // 16-byte band chunks a thread copies per pass
@@ -37,29 +40,62 @@ template <int M> __device__ __forceinline__ float4 realign(const float4 a, const
     return make_float4(a.w, b.x, b.y, b.z);
 }
 
-// One alignment group of the tile's windows: acc += elements(k) * x window.
 template <int M, class E>
-__device__ __forceinline__ void staged_group(const int *__restrict__ rec, int beg, int end,
-                                             unsigned long long mask, const E *__restrict__ ep,
-                                             unsigned S, const float4 *__restrict__ xs4,
-                                             unsigned tid, float (&acc)[4])
+__device__ __forceinline__ void stage_fma(const Vec<4, E> &e, const float4 *__restrict__ xs4,
+                                          int q, float (&acc)[4])
 {
-#pragma unroll 4
+  const float4 a = xs4[q];
+  const float4 b = M ? xs4[q + 1] : a;
+  const float4 xv = realign<M>(a, b);
+  acc[0] = fmaf(float(e.v[0]), xv.x, acc[0]);
+  acc[1] = fmaf(float(e.v[1]), xv.y, acc[1]);
+  acc[2] = fmaf(float(e.v[2]), xv.z, acc[2]);
+  acc[3] = fmaf(float(e.v[3]), xv.w, acc[3]);
+}
+
+// A group of a uniform tile: entry i names diagonal k directly.
+template <int M, class E>
+__device__ __forceinline__ void group_uniform(const int *__restrict__ rec, int beg, int end,
+                                              const E *__restrict__ ep, unsigned S,
+                                              const float4 *__restrict__ xs4, int tid,
+                                              float (&acc)[4])
+{
+  int i = beg;
+  for (; i + 4 <= end; i += 4) {
+    int vv[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      vv[j] = rec[32 + i + j];
+    Vec<4, E> e[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      e[j] = ld_stream<4>(ep + (size_t)(unsigned)(vv[j] >> 24) * S);
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      stage_fma<M>(e[j], xs4, ((vv[j] & 0xffffff) >> 2) + tid, acc);
+  }
+  for (; i < end; i++) {
+    const int v = rec[32 + i];
+    stage_fma<M>(ld_stream<4>(ep + (size_t)(unsigned)(v >> 24) * S), xs4,
+                 ((v & 0xffffff) >> 2) + tid, acc);
+  }
+}
+
+// A group of a tile whose slices differ: bit u of the slice's mask says
+// whether it has window u, its diagonal index is the rank of u in the mask.
+template <int M, class E>
+__device__ __forceinline__ void group_masked(const int *__restrict__ rec, int beg, int end,
+                                             unsigned long long mask, const E *__restrict__ ep,
+                                             unsigned S, const float4 *__restrict__ xs4, int tid,
+                                             float (&acc)[4])
+{
   for (int i = beg; i < end; i++) {
     const int v = rec[32 + i];
     const int u = v >> 24;
-    if (!((mask >> u) & 1ull))
-      continue;
-    const int k = __popcll(mask & ((1ull << u) - 1ull));
-    const Vec<4, E> e = ld_stream<4>(ep + (size_t)k * S);
-    const int q = ((v & 0xffffff) >> 2) + (int)tid;
-    const float4 a = xs4[q];
-    const float4 b = M ? xs4[q + 1] : a;
-    const float4 xv = realign<M>(a, b);
-    acc[0] = fmaf(float(e.v[0]), xv.x, acc[0]);
-    acc[1] = fmaf(float(e.v[1]), xv.y, acc[1]);
-    acc[2] = fmaf(float(e.v[2]), xv.z, acc[2]);
-    acc[3] = fmaf(float(e.v[3]), xv.w, acc[3]);
+    if ((mask >> u) & 1ull) {
+      const int k = __popcll(mask & ((1ull << u) - 1ull));
+      stage_fma<M>(ld_stream<4>(ep + (size_t)k * S), xs4, ((v & 0xffffff) >> 2) + tid, acc);
+    }
   }
 }
 
@@ -73,61 +109,49 @@ __global__ void __launch_bounds__(kStageThreads, 5)
   __shared__ __align__(16) int rec[kStageRecInts];
 
   const unsigned S = a.slice_height;
-  const unsigned tid = threadIdx.x;
+  const int tid = (int)threadIdx.x;
   const unsigned spt = kStageTileRows / S;
   const unsigned tile = blockIdx.x;
-  if (tid < (unsigned)kStageRecInts)
+  if (tid < kStageRecInts)
     rec[tid] = __ldg(recs + (size_t)tile * kStageRecInts + tid);
   // this thread's four rows: tile rows 4 tid .. 4 tid + 3 of slice s
-  const unsigned t0 = 4 * tid;
+  const unsigned t0 = 4u * (unsigned)tid;
   const unsigned s = t0 / S, r = t0 & (S - 1);
   const unsigned b = tile * spt + s;
   const bool act = b < a.n_slices;
   // slice header [elms_end, cols_end, diag_ptr] (conversion.h:393-402)
   const unsigned *h = a.sp + 3 * (size_t)(act ? b : tile * spt);
-  const unsigned e0 = __ldg(h), c0 = __ldg(h + 1), d0 = __ldg(h + 2);
+  const unsigned e0 = __ldg(h), c0 = __ldg(h + 1);
   const unsigned e1 = __ldg(h + 3), c1 = __ldg(h + 4);
-  const unsigned nell = act ? (c1 - c0) / S : 0u;
-  const unsigned nd = act ? (e1 - e0 - (c1 - c0)) / S : 0u;
   const E *__restrict__ ep = a.elms + e0 + (c1 - c0) + r;  // first diagonal element
 
   pdl_wait();
   if (a.skip && *a.skip)
     return;
   __syncthreads();  // rec
-  const bool staged = rec[0] && rec[2] <= a.stage_words;
+  const int kind = rec[2] <= a.stage_words ? rec[0] : 0;
   float acc[4] = {0.f, 0.f, 0.f, 0.f};
-  if (staged) {
-    // copy the bands: chunk g of the tile's concatenated bands, 16 bytes each
+  if (kind) {
+    // copy the bands, 16-byte chunks: chunk g lies in the band whose running
+    // total passes g
     const int nb = rec[1];
     const int n = (int)a.n_cols;
-    int nch_total = 0;
-    for (int q = 0; q < nb; q++) {
-      const int lo = rec[4 + 3 * q], hi = rec[5 + 3 * q];
-      const int c0q = lo >= 0 ? lo / 4 * 4 : -((-lo + 3) / 4) * 4;
-      nch_total += (hi - c0q + 3) / 4;
-    }
+    const int nch_total = rec[5 + 3 * (nb - 1)];
     for (int g0 = 0; g0 < nch_total; g0 += kStageThreads * kStageMaxChunks) {
       float4 v[kStageMaxChunks];
       int dst[kStageMaxChunks];
 #pragma unroll
       for (int i = 0; i < kStageMaxChunks; i++) {
-        const int g = g0 + i * kStageThreads + (int)tid;
+        const int g = g0 + i * kStageThreads + tid;
         dst[i] = -1;
         if (g >= nch_total)
           continue;
-        int q = 0, base = 0, c0q = 0, nch = 0;
-        for (;; q++) {
-          const int lo = rec[4 + 3 * q], hi = rec[5 + 3 * q];
-          c0q = lo >= 0 ? lo / 4 * 4 : -((-lo + 3) / 4) * 4;
-          nch = (hi - c0q + 3) / 4;
-          if (g < base + nch || q + 1 == nb)
-            break;
-          base += nch;
-        }
-        const int c = g - base;
-        const int col = c0q + c * 4;
-        dst[i] = rec[6 + 3 * q] - (rec[4 + 3 * q] - c0q) + c * 4;
+        int q = 0;
+        while (g >= rec[5 + 3 * q])
+          q++;
+        const int c = g - (q ? rec[5 + 3 * (q - 1)] : 0);
+        const int col = rec[4 + 3 * q] + 4 * c;
+        dst[i] = rec[6 + 3 * q] + 4 * c;
         if (a.x_al16 && col >= 0 && col + 4 <= n) {
           v[i] = __ldg(reinterpret_cast<const float4 *>(a.x + col));
         } else {
@@ -143,33 +167,45 @@ __global__ void __launch_bounds__(kStageThreads, 5)
           *reinterpret_cast<float4 *>(xs + dst[i]) = v[i];
     }
     __syncthreads();
-    const unsigned long long mask =
-        act ? ((unsigned long long)(unsigned)rec[97 + 2 * s] << 32) | (unsigned)rec[96 + 2 * s]
-            : 0ull;
-    staged_group<0>(rec, 0, rec[28], mask, ep, S, xs4, tid, acc);
-    staged_group<1>(rec, rec[28], rec[29], mask, ep, S, xs4, tid, acc);
-    staged_group<2>(rec, rec[29], rec[30], mask, ep, S, xs4, tid, acc);
-    staged_group<3>(rec, rec[30], rec[31], mask, ep, S, xs4, tid, acc);
-  } else {
+    if (kind == 1) {
+      if (act) {
+        group_uniform<0>(rec, 0, rec[28], ep, S, xs4, tid, acc);
+        group_uniform<1>(rec, rec[28], rec[29], ep, S, xs4, tid, acc);
+        group_uniform<2>(rec, rec[29], rec[30], ep, S, xs4, tid, acc);
+        group_uniform<3>(rec, rec[30], rec[31], ep, S, xs4, tid, acc);
+      }
+    } else {
+      const unsigned long long mask =
+          act ? ((unsigned long long)(unsigned)rec[97 + 2 * s] << 32) | (unsigned)rec[96 + 2 * s]
+              : 0ull;
+      group_masked<0>(rec, 0, rec[28], mask, ep, S, xs4, tid, acc);
+      group_masked<1>(rec, rec[28], rec[29], mask, ep, S, xs4, tid, acc);
+      group_masked<2>(rec, rec[29], rec[30], mask, ep, S, xs4, tid, acc);
+      group_masked<3>(rec, rec[30], rec[31], mask, ep, S, xs4, tid, acc);
+    }
+  } else if (act) {
     // read-only-path walk of the slice (kernel.h:80-92)
+    const unsigned nd = (e1 - e0 - (c1 - c0)) / S;
+    const unsigned d0 = __ldg(h + 2);
     const unsigned adj = r - S;
 #pragma unroll 2
     for (unsigned k = 0; k < nd; k++) {
       const Vec<4, E> e = ld_stream<4>(ep + (size_t)k * S);
       const unsigned base = __ldg(a.sp + d0 + k) + adj;
 #pragma unroll
-      for (int h = 0; h < 4; h++)
-        acc[h] = fmaf(float(e.v[h]), ld_x_guard(a.x, base + h, a.n_cols), acc[h]);
+      for (int j = 0; j < 4; j++)
+        acc[j] = fmaf(float(e.v[j]), ld_x_guard(a.x, base + j, a.n_cols), acc[j]);
     }
   }
   // entries off the slice's diagonals, with explicit columns (kernel.h:70-79)
-  for (unsigned j = 0; j < nell; j++) {
-    const size_t q = (size_t)j * S + r;
+  const unsigned nell = act ? (c1 - c0) / S : 0u;
+  for (unsigned jj = 0; jj < nell; jj++) {
+    const size_t q = (size_t)jj * S + r;
     const Vec<4, E> e = ld_stream<4>(a.elms + e0 + q);
     const Vec<4, unsigned> cc = ld_stream<4>(a.cols + c0 + q);
 #pragma unroll
-    for (int h = 0; h < 4; h++)
-      acc[h] = fmaf(float(e.v[h]), ld_x_guard(a.x, cc.v[h], a.n_cols), acc[h]);
+    for (int j = 0; j < 4; j++)
+      acc[j] = fmaf(float(e.v[j]), ld_x_guard(a.x, cc.v[j], a.n_cols), acc[j]);
   }
 
   pdl_trigger();
@@ -185,8 +221,8 @@ __global__ void __launch_bounds__(kStageThreads, 5)
         acc[3] = fmaf(dg.w, ld_x_guard(a.x, row + 3, a.n_cols), acc[3] * a.inv_scale);
       } else {
 #pragma unroll
-        for (int h = 0; h < 4; h++)
-          acc[h] *= a.inv_scale;
+        for (int j = 0; j < 4; j++)
+          acc[j] *= a.inv_scale;
       }
     }
   }
@@ -196,13 +232,14 @@ __global__ void __launch_bounds__(kStageThreads, 5)
     double dv = 0.0, dw = 0.0;
     const bool two = a.ep.out2 != nullptr;
     if (act) {
-      const float4 vv = *reinterpret_cast<const float4 *>(static_cast<const float *>(a.ep.v) + row);
+      const float4 vv =
+          *reinterpret_cast<const float4 *>(static_cast<const float *>(a.ep.v) + row);
       const float w[4] = {vv.x, vv.y, vv.z, vv.w};
 #pragma unroll
-      for (int h = 0; h < 4; h++) {
-        dv = fma((double)acc[h], (double)w[h], dv);
+      for (int j = 0; j < 4; j++) {
+        dv = fma((double)acc[j], (double)w[j], dv);
         if (two)
-          dw = fma((double)w[h], (double)w[h], dw);
+          dw = fma((double)w[j], (double)w[j], dw);
       }
     }
     if (two)

@@ -28,13 +28,14 @@ def check_records(B):
         assert 1 <= nb <= 8 and total % 4 == 0 and 1 <= nu <= 64
         # shared-memory word -> absolute x column, band by band as copied
         col_of = np.full(total, np.iinfo(np.int64).min)
+        prev = 0
         for q in range(nb):
-            lo, hi, off = r[4 + 3 * q], r[5 + 3 * q], r[6 + 3 * q]
-            assert off % 4 == lo % 4 and hi > lo
-            c0 = (lo // 4) * 4
-            nch = (hi - c0 + 3) // 4
-            dst0 = off - (lo - c0)
+            c0, run, dst0 = r[4 + 3 * q], r[5 + 3 * q], r[6 + 3 * q]
+            nch = run - prev
+            prev = run
+            assert c0 % 4 == 0 and nch >= 1
             assert dst0 >= 0 and dst0 % 4 == 0 and dst0 + nch * 4 <= total
+            assert np.all(col_of[dst0: dst0 + nch * 4] == np.iinfo(np.int64).min)  # no overlap
             col_of[dst0: dst0 + nch * 4] = c0 + np.arange(nch * 4)
         ends = [r[28 + m] for m in range(4)]
         assert ends == sorted(ends) and ends[3] == nu
@@ -52,6 +53,10 @@ def check_records(B):
             mask = (int(r[97 + 2 * s]) & 0xFFFFFFFF) << 32 | (int(r[96 + 2 * s]) & 0xFFFFFFFF)
             bits = [u for u in range(64) if mask >> u & 1]
             assert len(bits) == nd
+            if r[0] == 1:  # uniform tile: the kernel takes window u as diagonal k = u
+                assert bits == list(range(nu))
+            else:
+                assert r[0] == 2
             tid = (s * S + np.arange(0, S, 4)) // 4  # threads of the slice
             for k, u in enumerate(bits):
                 dp = int(sp[sp[3 * b + 2] + k])  # diag_pos: local row r reads x[dp + r - S]
