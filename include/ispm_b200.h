@@ -131,10 +131,15 @@ int ispm_dslell_upload(const ispm_slell *h, ispm_dslell **out);
 int ispm_dslell_upload_f16(const ispm_slell *h, ispm_dslell **out);
 /* Diagnostics of the staged SpMV walk (launch shape N = S, H = 1; no
  * counterpart in the reference): the tile records an upload of m computes
- * (224 ints per 1024-row tile; none unless m has diagonal blocks and a fixed
- * slice height dividing 1024).  *n_ints receives the count; at most cap ints
+ * (144 ints per 256-row tile; none unless m has diagonal blocks and a fixed
+ * slice height in [16, 256]).  *n_ints receives the count; at most cap ints
  * are written to out (which may be NULL with cap 0). */
 int ispm_slell_stage_records(const ispm_slell *m, int *out, long long cap, long long *n_ints);
+/* The staged walk's wait-timeout record: *code = 0, or the first timeout a
+ * staged launch met since the last call (1 a consumer warp's wait for a
+ * tile, 2 the copy warp's wait for a free slot, 3 the final wait for its
+ * copies); the record is cleared.  Synchronous. */
+int ispm_spmv_stage_fault(int *code);
 /* Re-upload only the element values of a matrix with unchanged structure
  * (plan/plan.h:39-42, implemented as the element-only H2D copy it means). */
 int ispm_dslell_update_elms(ispm_dslell *d, const ispm_slell *h);
@@ -174,7 +179,8 @@ int ispm_launch_spmv(int x_dtype, const ispm_launch_params *p, const ispm_slell_
  * ispm_csr_split_f16 converted with ispm_csr_to_slell and its element array
  * stored as binary16) and diag holds m->n_rows FP32 values (0 on padded
  * rows), 16-byte aligned.  This is the product the solver's matrix_f16 inner
- * iterations run; same launch parameters as ispm_launch_spmv. */
+ * iterations run; same launch parameters as ispm_launch_spmv.  diag NULL:
+ * y = inv_scale * (m x), an FP16-stored factor (the factor_f16 option). */
 int ispm_launch_spmv_split(const ispm_launch_params *p, const ispm_slell_view *m,
                            const float *diag, float inv_scale, const float *x, float *y,
                            void *stream);

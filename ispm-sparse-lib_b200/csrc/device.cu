@@ -52,7 +52,7 @@ void stage_records(const HostSlell &h, std::vector<int> &rec)
   const unsigned S = h.slice_height;
   if (!h.diags || h.var_height || h.hblock != 1 || S < 16 || kStageTileRows % S || !h.n_slices)
     return;
-  const unsigned spt = kStageTileRows / S;  // <= 64 slices per tile
+  const unsigned spt = kStageTileRows / S;  // <= 16 slices per tile
   const unsigned n_tiles = (h.n_slices + spt - 1) / spt;
   rec.assign((size_t)n_tiles * kStageRecInts, 0);
   const unsigned *sp = h.slice_ptr.data();
@@ -61,19 +61,21 @@ void stage_records(const HostSlell &h, std::vector<int> &rec)
   for (unsigned t = 0; t < n_tiles; t++) {
     int *r = rec.data() + (size_t)t * kStageRecInts;
     const unsigned b0 = t * spt, nsl = std::min(spt, h.n_slices - b0);
+    r[2] = (int)nsl;
     // window starts of every slice's diagonals (slice b: [elms_end, cols_end,
     // diag_ptr] at 3b, conversion.h:393-402): the x column that tile row 0
     // would read, so x[w + t] serves tile row t (diag_pos is absolute)
     all.clear();
-    bool ascending = true;
+    bool ok = true, ell = false;
     for (unsigned s = 0; s < nsl; s++) {
       const unsigned b = b0 + s;
       const unsigned e0 = sp[3 * b], c0 = sp[3 * b + 1], e1 = sp[3 * b + 3], c1 = sp[3 * b + 4];
+      ell = ell || c1 != c0;
       const unsigned nd = (e1 - e0 - (c1 - c0)) / S, dd = sp[3 * b + 2];
       for (unsigned k = 0; k < nd; k++) {
         const long long w = (long long)sp[dd + k] - S - (long long)s * S;
         if (k && w <= all.back())
-          ascending = false;
+          ok = false;
         all.push_back(w);
       }
     }
@@ -81,9 +83,11 @@ void stage_records(const HostSlell &h, std::vector<int> &rec)
     std::sort(win.begin(), win.end());
     win.erase(std::unique(win.begin(), win.end()), win.end());
     const int nu = (int)win.size();
-    if (!ascending || nu < 1 || nu > kStageMaxDiag)
-      continue;  // r[0] = 0: the tile reads x directly
-    // runs of window starts less than rows + gap apart share a band
+    const long long e_first = sp[3 * b0], e_count = (long long)sp[3 * (b0 + nsl)] - e_first;
+    if (!ok || nu < 1 || nu > kStageMaxDiag || e_first > INT32_MAX || e_count > INT32_MAX)
+      continue;  // r[0] = 0
+    // runs of window starts less than rows + gap apart share a band; a band
+    // covers its windows' columns for all tile rows, 16-byte aligned
     long long lo[kStageMaxDiag], hi[kStageMaxDiag];
     int band[kStageMaxDiag], nb = 0;
     for (int u = 0; u < nu; u++) {
@@ -97,61 +101,46 @@ void stage_records(const HostSlell &h, std::vector<int> &rec)
     }
     if (nb > kStageMaxBands || lo[0] < INT32_MIN / 2 || hi[nb - 1] > INT32_MAX / 2)
       continue;
-    // shared-memory placement: column c sits at a word congruent to c
-    // modulo 4, so 16-byte chunks of x land on 16-byte chunks
-    long long off = 0, offs[kStageMaxBands];
+    long long words = 0, dst[kStageMaxBands], c0[kStageMaxBands];
     for (int q = 0; q < nb; q++) {
-      off = (off + 3) / 4 * 4 + (((lo[q] % 4) + 4) % 4);
-      offs[q] = off;
-      off += hi[q] - lo[q];
+      c0[q] = lo[q] >= 0 ? lo[q] / 4 * 4 : -((-lo[q] + 3) / 4) * 4;
+      const long long c1 = (hi[q] + 3) / 4 * 4;
+      dst[q] = words;
+      r[156 + 2 * q] = (int)c0[q];
+      r[157 + 2 * q] = (int)(c1 - c0[q]);
+      words += c1 - c0[q];
     }
-    const long long total = (off + 3) / 4 * 4;
-    if (total >= (1 << 24))
+    if (words > kStageMaxXWords)
       continue;
-    r[1] = nb;
-    r[2] = (int)total;
-    r[3] = nu;
-    long long chunks = 0;
-    for (int q = 0; q < nb; q++) {
-      const long long c0 = lo[q] >= 0 ? lo[q] / 4 * 4 : -((-lo[q] + 3) / 4) * 4;
-      chunks += (hi[q] - c0 + 3) / 4;
-      r[4 + 3 * q] = (int)c0;
-      r[5 + 3 * q] = (int)chunks;
-      r[6 + 3 * q] = (int)(offs[q] - (lo[q] - c0));
-    }
-    // uniform: every slice has all nu windows (so its k-th diagonal is window k)
-    bool all_slices = true;
-    for (unsigned s = 0; s < nsl && all_slices; s++) {
-      const unsigned b = b0 + s;
-      const unsigned e0 = sp[3 * b], c0 = sp[3 * b + 1], e1 = sp[3 * b + 3], c1 = sp[3 * b + 4];
-      all_slices = (int)((e1 - e0 - (c1 - c0)) / S) == nu;
-    }
-    r[0] = all_slices ? 1 : 2;
-    // entries grouped by the shared-memory start modulo 4
-    int i = 0;
-    for (int m = 0; m < 4; m++) {
-      for (int u = 0; u < nu; u++) {
-        const int q = band[u];
-        const long long sx = offs[q] + (win[u] - lo[q]);
-        if ((sx & 3) == m)
-          r[32 + i++] = (int)sx | (u << 24);
-      }
-      r[28 + m] = i;
-    }
-    // slice masks over the window starts
+    r[1] = nu;
+    for (int u = 0; u < nu; u++)
+      r[8 + u] = (int)(dst[band[u]] + (win[u] - c0[band[u]]));
+    // slice masks over the window starts, slice element offsets; uniform
+    // when every slice carries all nu windows and no explicit columns
+    bool uniform = !ell;
     for (unsigned s = 0; s < nsl; s++) {
       const unsigned b = b0 + s;
-      const unsigned e0 = sp[3 * b], c0 = sp[3 * b + 1], e1 = sp[3 * b + 3], c1 = sp[3 * b + 4];
-      const unsigned nd = (e1 - e0 - (c1 - c0)) / S, dd = sp[3 * b + 2];
+      const unsigned e0 = sp[3 * b], c0s = sp[3 * b + 1], e1 = sp[3 * b + 3],
+                     c1s = sp[3 * b + 4];
+      const unsigned nd = (e1 - e0 - (c1s - c0s)) / S, dd = sp[3 * b + 2];
       unsigned long long mask = 0;
       for (unsigned k = 0; k < nd; k++) {
         const long long w = (long long)sp[dd + k] - S - (long long)s * S;
         const int u = (int)(std::lower_bound(win.begin(), win.end(), w) - win.begin());
         mask |= 1ull << u;
       }
-      r[96 + 2 * s] = (int)(unsigned)(mask & 0xffffffffull);
-      r[97 + 2 * s] = (int)(unsigned)(mask >> 32);
+      uniform = uniform && (int)nd == nu;
+      r[72 + 2 * s] = (int)(unsigned)(mask & 0xffffffffull);
+      r[73 + 2 * s] = (int)(unsigned)(mask >> 32);
+      r[104 + s] = (int)((long long)e0 + (c1s - c0s) - e_first);
+      r[120 + s] = (int)((c1s - c0s) / S);
+      r[136 + s] = (int)c0s;
     }
+    r[0] = uniform ? 1 : 2;
+    r[152] = (int)e_first;
+    r[153] = (int)e_count;
+    r[154] = nb;
+    r[155] = (int)words;
   }
 }
 
@@ -159,7 +148,8 @@ void stage_records(const HostSlell &h, std::vector<int> &rec)
 namespace {
 struct StageEntry {
   const int *rec;
-  int max_words;
+  int max_x_words;
+  int max_elms;
   unsigned n_slices;
 };
 std::mutex g_stage_mu;
@@ -172,7 +162,8 @@ bool find_stage_records(const unsigned *slice_ptr, unsigned n_slices, StageInfo 
   for (const auto &e : g_stage)
     if (e.first == slice_ptr && e.second.n_slices == n_slices) {
       out.rec = e.second.rec;
-      out.max_words = e.second.max_words;
+      out.max_x_words = e.second.max_x_words;
+      out.max_elms = e.second.max_elms;
       return true;
     }
   return false;
@@ -184,10 +175,12 @@ int DeviceSlell::attach_stage_records(const HostSlell &h)
   stage_records(h, rec);
   if (rec.empty())
     return ISPM_OK;
-  int mx = 0;
+  int mx = 0, me = 0;
   for (size_t t = 0; t < rec.size(); t += kStageRecInts)
-    if (rec[t])
-      mx = std::max(mx, rec[t + 2]);
+    if (rec[t]) {
+      mx = std::max(mx, rec[t + 155]);
+      me = std::max(me, rec[t + 153]);
+    }
   cudaError_t e = cudaMalloc(&stage_rec, rec.size() * sizeof(int));
   if (e != cudaSuccess) {
     stage_rec = nullptr;
@@ -197,9 +190,8 @@ int DeviceSlell::attach_stage_records(const HostSlell &h)
   }
   ISPM_CUDA_TRY(cudaMemcpy(stage_rec, rec.data(), rec.size() * sizeof(int),
                            cudaMemcpyHostToDevice));
-  stage_max_words = mx;
   std::lock_guard<std::mutex> g(g_stage_mu);
-  g_stage.push_back({slice_ptr, StageEntry{stage_rec, mx, meta.n_slices}});
+  g_stage.push_back({slice_ptr, StageEntry{stage_rec, mx, me, meta.n_slices}});
   return ISPM_OK;
 }
 
@@ -216,7 +208,6 @@ void DeviceSlell::release()
     }
     cudaFree(stage_rec);
     stage_rec = nullptr;
-    stage_max_words = 0;
   }
   if (slice_ptr)
     cudaFree(slice_ptr);

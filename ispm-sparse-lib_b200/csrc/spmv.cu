@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <type_traits>
 
 #include "cuda_util.cuh"
@@ -52,7 +53,9 @@ template <class T, class E> struct SpmvArgs {
   int pdl;            // launched as a programmatic dependent of the previous kernel
   const float *dg;    // split operators (E = __half): FP32 diagonal, one per row
   float inv_scale;    // split operators: 1 / the power-of-two element scale
-  int stage_words;    // staged walk: x staging capacity (values of T) per CTA
+  int st_slots;       // staged walk: ring slots, bytes per slot, x area offset in a slot
+  int st_slot_bytes;
+  int st_x_off;
 };
 
 // Finish a fused dot product: every block publishes its partial, the last
@@ -207,6 +210,32 @@ __device__ __forceinline__ void load_window(const T *__restrict__ x, unsigned ba
         T r = w[h];
 #pragma unroll
         for (int k = 1; k < H; k++)
+          r = sh == (unsigned)k ? w[h + k] : r;
+        xv[h] = r;
+      }
+      return;
+    }
+  } else if constexpr (H == 8 && sizeof(T) == 4) {
+    // eight FP32 rows a thread (16-bit elements: one 128-bit element load):
+    // two aligned 128-bit loads, three when base is not 4-aligned
+    const unsigned sh = base & 3u;
+    const unsigned a0 = base - sh;
+    if (vec_ok && a0 < n && n - a0 >= (sh ? 12u : 8u)) {
+      T w[12];
+      *reinterpret_cast<float4 *>(w) = __ldg(reinterpret_cast<const float4 *>(x + a0));
+      *reinterpret_cast<float4 *>(w + 4) = __ldg(reinterpret_cast<const float4 *>(x + a0 + 4));
+      if (sh) {
+        *reinterpret_cast<float4 *>(w + 8) = __ldg(reinterpret_cast<const float4 *>(x + a0 + 8));
+      } else {
+#pragma unroll
+        for (int k = 8; k < 12; k++)
+          w[k] = T(0);
+      }
+#pragma unroll
+      for (int h = 0; h < 8; h++) {
+        T r = w[h];
+#pragma unroll
+        for (int k = 1; k < 4; k++)
           r = sh == (unsigned)k ? w[h + k] : r;
         xv[h] = r;
       }
@@ -507,7 +536,7 @@ int launch_te(const ispm_launch_params &p, const ispm_slell_view &m, const void 
   a.pdl = pdl ? 1 : 0;
   a.dg = nullptr;
   a.inv_scale = 1.f;
-  a.stage_words = 0;
+  a.st_slots = a.st_slot_bytes = a.st_x_off = 0;
   if constexpr (std::is_same<E, __half>::value) {
     if (!split || (split->diag && !aligned(split->diag, 16)))
       return fail(ISPM_ERR_INVALID,
@@ -542,13 +571,26 @@ int launch_te(const ispm_launch_params &p, const ispm_slell_view &m, const void 
     return fail(ISPM_ERR_INVALID, "matrix arrays or y not aligned to H=%u elements", p.H);
   if constexpr (std::is_same<T, float>::value) {
     StageInfo si;
-    if (!ln && (!ep || !ep->out || aligned(ep->v, 16)) && staged_shape(ISPM_F32, p, m, y, si))
+    if (!ln && staged_shape(ISPM_F32, p, m, x, si, a.st_slots, a.st_slot_bytes, a.st_x_off))
       return launch_staged<E>(a, si, s);
   }
   switch (p.H) {
   case 1: return launch_h<T, E, 1>(a, m, p.N, s, ln != nullptr);
   case 2: return launch_h<T, E, 2>(a, m, p.N, s, ln != nullptr);
   case 4: return launch_h<T, E, 4>(a, m, p.N, s, ln != nullptr);
+  case 8:
+    // eight rows a thread: FP32 vectors, one column per stored index
+    if constexpr (std::is_same<T, float>::value) {
+      if (ln || m.hblock != 1)
+        return fail(ISPM_ERR_INVALID, "H = 8 needs hblock 1 and a single system");
+      const bool V = m.var_height != 0, D = m.diags != 0;
+      if (V)
+        return D ? launch_one<T, E, 8, 1, true, true>(a, p.N, s)
+                 : launch_one<T, E, 8, 1, true, false>(a, p.N, s);
+      return D ? launch_one<T, E, 8, 1, false, true>(a, p.N, s)
+               : launch_one<T, E, 8, 1, false, false>(a, p.N, s);
+    }
+    return fail(ISPM_ERR_INVALID, "H = 8 needs FP32 vectors");
   }
   return fail(ISPM_ERR_INVALID, "H %u", p.H);
 }
@@ -569,8 +611,10 @@ int check_launch(int x_dtype, const ispm_launch_params &p, const ispm_slell_view
                                 : "bfloat16");
   if (!is_pow2(p.N) || p.N < 4 || p.N > 1024)
     return fail(ISPM_ERR_INVALID, "N = %u (power of two in [4, 1024])", p.N);
-  if (p.H != 1 && p.H != 2 && p.H != 4)
-    return fail(ISPM_ERR_INVALID, "H = %u (1, 2 or 4)", p.H);
+  if (p.H != 1 && p.H != 2 && p.H != 4 && p.H != 8)
+    return fail(ISPM_ERR_INVALID, "H = %u (1, 2, 4, or 8 with FP32 vectors)", p.H);
+  if (p.H == 8 && (x_dtype != ISPM_F32 || m.hblock != 1))
+    return fail(ISPM_ERR_INVALID, "H = 8 needs FP32 vectors and hblock 1");
   if (!(p.N >= p.S / p.H && p.S >= p.H))
     return fail(ISPM_ERR_INVALID, "launch params fail N >= S/H && S >= H");
   if (m.hblock != 1 && m.hblock != 2 && m.hblock != 4)
@@ -687,13 +731,26 @@ int ispm_launch_spmv_split(const ispm_launch_params *p, const ispm_slell_view *m
                            void *stream)
 {
   ispm::clear_error();
-  if (!p || !m || !diag)
-    return ispm::fail(ISPM_ERR_INVALID, "NULL params, matrix or diagonal");
+  if (!p || !m)
+    return ispm::fail(ISPM_ERR_INVALID, "NULL params or matrix");
   if (m->elm_dtype != ISPM_F16)
     return ispm::fail(ISPM_ERR_INVALID, "the split product takes FP16 elements");
   ispm::SpmvSplit sp{diag, inv_scale};
   return ispm::launch_spmv(ISPM_F32, *p, *m, x, y, (cudaStream_t)stream, nullptr, nullptr,
                            false, &sp);
+}
+
+int ispm_spmv_stage_fault(int *code)
+{
+  ispm::clear_error();
+  if (!code)
+    return ispm::fail(ISPM_ERR_INVALID, "NULL code");
+  unsigned v = 0;
+  const unsigned zero = 0;
+  ISPM_CUDA_TRY(cudaMemcpyFromSymbol(&v, ispm::g_stage_fault, sizeof v));
+  ISPM_CUDA_TRY(cudaMemcpyToSymbol(ispm::g_stage_fault, &zero, sizeof zero));
+  *code = (int)v;
+  return ISPM_OK;
 }
 
 }  // extern "C"

@@ -64,18 +64,21 @@ struct SpmvSplit {
 };
 
 // Tile records of the device matrix whose slice_ptr array is `slice_ptr`
-// (registered by DeviceSlell uploads, dropped on release) and the largest
-// staged-band footprint (shared-memory words) over its tiles.
+// (registered by DeviceSlell uploads, dropped on release), the largest x
+// area (words) and element count over its staged tiles.
 struct StageInfo {
   const int *rec = nullptr;
-  int max_words = 0;
+  int max_x_words = 0;
+  int max_elms = 0;
 };
 bool find_stage_records(const unsigned *slice_ptr, unsigned n_slices, StageInfo &out);
 
 // Validate and launch y = A x on `s`.  `skip` (device int, may be NULL): the
 // kernel returns at once when it holds a nonzero value.
 // pdl: launch as a programmatic dependent of the stream's previous kernel
-// (that kernel's results are read only after it completed).
+// (that kernel's results are read only after it completed; the matrix must
+// be final before that kernel started, since the staged walk fetches its
+// elements before the wait).
 int launch_spmv(int x_dtype, const ispm_launch_params &p, const ispm_slell_view &m,
                 const void *x, void *y, cudaStream_t s, const int *skip = nullptr,
                 const SpmvDot *ep = nullptr, bool pdl = false,
@@ -94,29 +97,40 @@ unsigned spmv_cta_rows(const ispm_launch_params &p, const ispm_slell_view &m);
 // kStageRecInts ints, computed on the host from the slice records when a
 // diagonal-block matrix of fixed slice height is uploaded.  A diagonal of
 // slice s at diag_pos d serves tile row t = s S + r from x[w + t] with the
-// window start w = d - S - s S; the tile's windows are the union W of those
-// starts over its slices (ascending, u = 0 .. nu - 1):
-//   [0] 0: not staged; 1: staged, every slice carries all nu windows, in
-//       order (then u is the slice's diagonal index k); 2: staged, slices
-//       differ (the masks below name each slice's diagonals).  Staged tiles
-//       have 1..64 window starts, every slice's diagonals in ascending
-//       order, at most 8 bands;
-//   [1] nb, the number of x bands (runs of nearby windows);
-//   [2] shared-memory words the bands take (16-byte chunk aligned);
-//   [3] nu, the number of window starts;
-//   [4 + 3q .. 6 + 3q] band q as the CTA copies it: first x column of its
-//       first 16-byte chunk (a multiple of 4), running total of chunks
-//       through band q, shared-memory word of its first chunk;
-//   [28 + m] end of group m (m = 0..3) in the entry list: the windows whose
-//       shared-memory start is congruent to m modulo 4;
-//   [32 + i] entry i: shared-memory word of x[w_u] | u << 24, grouped by m;
-//   [96 + 2s], [97 + 2s] slice s of the tile: bit u of this 64-bit mask is
-//       set when the slice has a diagonal at window u (its k-th diagonal is
-//       its k-th set bit).
-constexpr unsigned kStageTileRows = 1024;
-constexpr int kStageRecInts = 224;
+// window start w = d - S - s S; the tile's windows are the union of those
+// starts over its slices (ascending, u = 0 .. nu - 1), merged into bands of
+// x that a copy engine moves into shared memory beside the tile's elements
+// (all of them: a tile's slices are consecutive in elms).  Ints [0, 152)
+// travel to shared memory with the tile (the compute side), [152, 172) are
+// the copy list the issuing warp reads:
+//   [0] 0: not staged (the tile reads everything from global memory);
+//       1: staged, every slice carries all nu windows in order (its k-th
+//       diagonal is window k) and no explicit-column entries; 2: staged,
+//       slices differ (masks below) or carry explicit-column entries.
+//       Staged tiles have 1..64 window starts, every slice's diagonals in
+//       ascending order and at most 8 bands;
+//   [1] nu; [2] slices in the tile; [3..8) 0;
+//   [8 + u] x-area word of x[w_u] (tile row t reads word [8 + u] + t);
+//   [72 + 2s], [73 + 2s] slice s: bit u of this 64-bit mask is set when the
+//       slice has a diagonal at window u (its k-th diagonal is its k-th set
+//       bit);
+//   [104 + s] slice s: offset of its first diagonal element from the tile's
+//       first element;
+//   [120 + s] slice s: explicit-column entries per row (its first element
+//       sits that many times S before its first diagonal element);
+//   [136 + s] slice s: its cols_end record (first column index, into cols);
+//   [152] the tile's first element (index into elms), [153] its element
+//       count; [154] nb, the number of bands; [155] x-area words;
+//   [156 + 2q], [157 + 2q] band q: first x column (a multiple of 4, may be
+//       negative), words (a multiple of 4); band q fills the x-area words
+//       after bands 0 .. q-1; columns outside x read zero.
+constexpr unsigned kStageTileRows = 256;
+constexpr int kStageRecInts = 176;
+constexpr int kStageRecComputeInts = 152;  // the part that travels with the tile
 constexpr int kStageMaxBands = 8;
 constexpr int kStageMaxDiag = 64;
+constexpr int kStageMaxSlices = 16;        // slice height >= 16
+constexpr int kStageMaxXWords = 8192;      // larger x areas are not staged
 constexpr int kStageGap = 32;  // windows this close (in words) share a band
 
 // Tile records of h (empty unless h is diagonal-block, fixed height, and its
@@ -129,7 +143,6 @@ struct DeviceSlell {
   unsigned *cols = nullptr;
   void *elms = nullptr;
   int *stage_rec = nullptr;  // tile records of the staged walk (device), or NULL
-  int stage_max_words = 0;
   // build, upload and register the tile records of h (no-op for other shapes)
   int attach_stage_records(const HostSlell &h);
   ispm_slell_view view() const

@@ -3,245 +3,395 @@
 // Included by spmv.cu (uses its SpmvArgs and fused-dot finishers).
 //
 // In the reference walk (cuda/spmv/kernel.h:80-92) the thread of local row r
-// reads x[diag_pos + r - S] for every diagonal of its slice.  Here a CTA of
-// 256 threads takes a tile of kStageTileRows = 1024 rows, each thread four
-// consecutive rows of one slice, so every element load is one 16-byte (FP32)
-// or 8-byte (FP16 / BF16) vector of a diagonal's column-major block.  The
-// tile's x windows -- the window starts w of all its slices' diagonals, x[w
-// + t] serving tile row t -- are merged into bands that the CTA copies into
-// shared memory once (16-byte loads, zero outside x).  A thread's four x
-// values then sit in two aligned 16-byte shared-memory chunks, shifted by
-// the window's start modulo 4; the host groups the windows by that shift, so
-// each group's realignment is fixed at compile time.  In the common tile,
-// every slice carries every window and an entry names the diagonal
-// directly, so the element loads of a group are independent and the
-// compiler batches them; tiles whose slices differ (grid faces) take a mask
-// per slice over the tile's windows (its k-th diagonal is its k-th set
-// bit).  All of this is computed on the host when the matrix is uploaded
-// (stage_records), so a CTA's set-up is one coalesced load of its record
-// beside its slice header.  Tiles with more than 64 windows, more than 8
-// bands or bands beyond the buffer read x through the read-only path with
-// bounds tests.
+// reads x[diag_pos + r - S] for every diagonal of its slice, two dependent
+// loads per element on the critical path.  Here the GPU's copy engine feeds
+// the FMAs: a persistent CTA per SM takes a contiguous run of 256-row tiles;
+// one producer warp moves each tile's record, its elements (one contiguous
+// range: staged tiles have diagonal blocks only) and the bands of x its
+// windows read (zero outside x) into a ring of shared-memory slots with bulk
+// asynchronous copies (cp.async.bulk) completing on an mbarrier per slot;
+// four consumer warps take the tiles in turn, each lane eight rows (t = lane
+// + 32 j), reading every element and x value from shared memory with
+// conflict-free 32-bit loads, and hand the slot back through a second
+// mbarrier.  The element copies of the first slots go out before the
+// programmatic-launch wait (the matrix is final before the previous kernel
+// starts), the x copies after it.  The producer keeps up to `slots` tiles in
+// flight, so the bytes in flight per SM are set by shared memory, not by
+// registers or warps.
+//
+// Every wait on an mbarrier is bounded (about 2^31 clock cycles): on a
+// timeout the CTA records a fault code in g_stage_fault, stops issuing and
+// waiting, and the producer waits (bounded) for the copies it issued before
+// the CTA exits.  The host reads and clears the code with
+// ispm_spmv_stage_fault().
 
-constexpr int kStageThreads = 256;
-constexpr int kStageMaxChunks = 4;  // 16-byte band chunks a thread copies per pass
+constexpr int kStageConsumers = 4;                     // compute warps
+constexpr int kStageThreads = 32 * (kStageConsumers + 1);
+constexpr int kStageMaxSlots = 8;
+constexpr int kStageSmemBudget = 220 * 1024;           // dynamic shared memory for the ring
+constexpr int kStageRecBytes = kStageRecComputeInts * 4;
 
-// x[w + t .. w + t + 3] from the two chunks holding it (shift M = (smem
-// start of x[w + t]) mod 4)
-template <int M> __device__ __forceinline__ float4 realign(const float4 a, const float4 b)
+__device__ unsigned g_stage_fault;  // 0, or the first timeout's code (1 consumer, 2 producer, 3 drain)
+
+__device__ __forceinline__ unsigned smem_u32(const void *p)
 {
-  if constexpr (M == 0)
-    return a;
-  else if constexpr (M == 1)
-    return make_float4(a.y, a.z, a.w, b.x);
-  else if constexpr (M == 2)
-    return make_float4(a.z, a.w, b.x, b.y);
-  else
-    return make_float4(a.w, b.x, b.y, b.z);
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned b, unsigned count)
+{
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(b), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned b, unsigned bytes)
+{
+  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(b), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned b, unsigned bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(b),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned b)
+{
+  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(b) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned b, unsigned parity)
+{
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n"
+      " mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(b), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Phase `parity` of barrier b completed: true; false once about 2^31 clock
+// cycles passed or (abort != NULL) the CTA gave up.
+__device__ __forceinline__ bool mbar_wait(unsigned b, unsigned parity, const volatile int *abort)
+{
+  if (mbar_try_wait(b, parity))
+    return true;
+  const long long t0 = clock64();
+  for (;;) {
+    if (mbar_try_wait(b, parity))
+      return true;
+    if ((abort && *abort) || clock64() - t0 > (1ll << 31))
+      return false;
+  }
+}
+// Global -> shared bulk copy completing `bytes` on barrier b (16-byte
+// aligned addresses, bytes a multiple of 16).
+__device__ __forceinline__ void bulk_g2s(unsigned dst, const void *src, unsigned bytes, unsigned b)
+{
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(dst),
+      "l"(src), "r"(bytes), "r"(b)
+      : "memory");
 }
 
-template <int M, class E>
-__device__ __forceinline__ void stage_fma(const Vec<4, E> &e, const float4 *__restrict__ xs4,
-                                          int q, float (&acc)[4])
+__device__ __forceinline__ void stage_fault(unsigned code, volatile int *abort)
 {
-  const float4 a = xs4[q];
-  const float4 b = M ? xs4[q + 1] : a;
-  const float4 xv = realign<M>(a, b);
-  acc[0] = fmaf(float(e.v[0]), xv.x, acc[0]);
-  acc[1] = fmaf(float(e.v[1]), xv.y, acc[1]);
-  acc[2] = fmaf(float(e.v[2]), xv.z, acc[2]);
-  acc[3] = fmaf(float(e.v[3]), xv.w, acc[3]);
-}
-
-// A group of a uniform tile: entry i names diagonal k directly.
-template <int M, class E>
-__device__ __forceinline__ void group_uniform(const int *__restrict__ rec, int beg, int end,
-                                              const E *__restrict__ ep, unsigned S,
-                                              const float4 *__restrict__ xs4, int tid,
-                                              float (&acc)[4])
-{
-  int i = beg;
-  for (; i + 4 <= end; i += 4) {
-    int vv[4];
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-      vv[j] = rec[32 + i + j];
-    Vec<4, E> e[4];
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-      e[j] = ld_stream<4>(ep + (size_t)(unsigned)(vv[j] >> 24) * S);
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-      stage_fma<M>(e[j], xs4, ((vv[j] & 0xffffff) >> 2) + tid, acc);
-  }
-  for (; i < end; i++) {
-    const int v = rec[32 + i];
-    stage_fma<M>(ld_stream<4>(ep + (size_t)(unsigned)(v >> 24) * S), xs4,
-                 ((v & 0xffffff) >> 2) + tid, acc);
-  }
-}
-
-// A group of a tile whose slices differ: bit u of the slice's mask says
-// whether it has window u, its diagonal index is the rank of u in the mask.
-template <int M, class E>
-__device__ __forceinline__ void group_masked(const int *__restrict__ rec, int beg, int end,
-                                             unsigned long long mask, const E *__restrict__ ep,
-                                             unsigned S, const float4 *__restrict__ xs4, int tid,
-                                             float (&acc)[4])
-{
-  for (int i = beg; i < end; i++) {
-    const int v = rec[32 + i];
-    const int u = v >> 24;
-    if ((mask >> u) & 1ull) {
-      const int k = __popcll(mask & ((1ull << u) - 1ull));
-      stage_fma<M>(ld_stream<4>(ep + (size_t)k * S), xs4, ((v & 0xffffff) >> 2) + tid, acc);
-    }
-  }
+  atomicCAS(&g_stage_fault, 0u, code);
+  *abort = 1;
 }
 
 template <class E>
-__global__ void __launch_bounds__(kStageThreads, 5)
+__global__ void __launch_bounds__(kStageThreads, 1)
     slell_spmv_staged_kernel(SpmvArgs<float, E> a, const int *__restrict__ recs)
 {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  float *xs = reinterpret_cast<float *>(smem_raw);
-  const float4 *xs4 = reinterpret_cast<const float4 *>(smem_raw);
-  __shared__ __align__(16) int rec[kStageRecInts];
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) unsigned long long full_bar[kStageMaxSlots];
+  __shared__ __align__(8) unsigned long long empty_bar[kStageMaxSlots];
+  __shared__ int abort_flag;
+  volatile int *abort = &abort_flag;
 
-  const unsigned S = a.slice_height;
-  const int tid = (int)threadIdx.x;
-  const unsigned spt = kStageTileRows / S;
-  const unsigned tile = blockIdx.x;
-  if (tid < kStageRecInts)
-    rec[tid] = __ldg(recs + (size_t)tile * kStageRecInts + tid);
-  // this thread's four rows: tile rows 4 tid .. 4 tid + 3 of slice s
-  const unsigned t0 = 4u * (unsigned)tid;
-  const unsigned s = t0 / S, r = t0 & (S - 1);
-  const unsigned b = tile * spt + s;
-  const bool act = b < a.n_slices;
-  // slice header [elms_end, cols_end, diag_ptr] (conversion.h:393-402)
-  const unsigned *h = a.sp + 3 * (size_t)(act ? b : tile * spt);
-  const unsigned e0 = __ldg(h), c0 = __ldg(h + 1);
-  const unsigned e1 = __ldg(h + 3), c1 = __ldg(h + 4);
-  const E *__restrict__ ep = a.elms + e0 + (c1 - c0) + r;  // first diagonal element
+  const int warp = (int)(threadIdx.x >> 5), lane = (int)(threadIdx.x & 31);
+  const unsigned S = a.slice_height, spt = kStageTileRows / S;
+  const unsigned n_tiles = (a.n_slices + spt - 1) / spt;
+  const unsigned t_beg = (unsigned)((unsigned long long)blockIdx.x * n_tiles / gridDim.x);
+  const unsigned t_end = (unsigned)((unsigned long long)(blockIdx.x + 1) * n_tiles / gridDim.x);
+  const unsigned cnt = t_end - t_beg;
+  const unsigned NS = (unsigned)a.st_slots, slot_bytes = (unsigned)a.st_slot_bytes;
+  const unsigned x_off = (unsigned)a.st_x_off;
+  const unsigned ring = smem_u32(smem);
+  if (threadIdx.x == 0) {
+    for (unsigned s = 0; s < NS; s++) {
+      mbar_init(smem_u32(&full_bar[s]), 1);
+      mbar_init(smem_u32(&empty_bar[s]), 1);
+    }
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
 
-  pdl_wait();
-  if (a.skip && *a.skip)
-    return;
-  __syncthreads();  // rec
-  const int kind = rec[2] <= a.stage_words ? rec[0] : 0;
-  float acc[4] = {0.f, 0.f, 0.f, 0.f};
-  if (kind) {
-    // copy the bands, 16-byte chunks: chunk g lies in the band whose running
-    // total passes g
-    const int nb = rec[1];
-    const int n = (int)a.n_cols;
-    const int nch_total = rec[5 + 3 * (nb - 1)];
-    for (int g0 = 0; g0 < nch_total; g0 += kStageThreads * kStageMaxChunks) {
-      float4 v[kStageMaxChunks];
-      int dst[kStageMaxChunks];
+  double dv = 0.0, dw = 0.0;
+  const bool two = a.ep.out2 != nullptr;
+  if (warp == kStageConsumers) {
+    // ---- producer ----------------------------------------------------------
+    // copy lists: lane l holds the one of tile (batch base + l); this batch
+    // in cl, the next one in nx
+    int cl[20], nx[20];
+    auto load_cl = [&](int(&d)[20], unsigned base) {
+      const unsigned tl = t_beg + base + (unsigned)lane;
+      if (tl < t_end) {
+        const int4 *p = reinterpret_cast<const int4 *>(recs + (size_t)tl * kStageRecInts +
+                                                       kStageRecComputeInts);
 #pragma unroll
-      for (int i = 0; i < kStageMaxChunks; i++) {
-        const int g = g0 + i * kStageThreads + tid;
-        dst[i] = -1;
-        if (g >= nch_total)
-          continue;
-        int q = 0;
-        while (g >= rec[5 + 3 * q])
-          q++;
-        const int c = g - (q ? rec[5 + 3 * (q - 1)] : 0);
-        const int col = rec[4 + 3 * q] + 4 * c;
-        dst[i] = rec[6 + 3 * q] + 4 * c;
-        if (a.x_al16 && col >= 0 && col + 4 <= n) {
-          v[i] = __ldg(reinterpret_cast<const float4 *>(a.x + col));
-        } else {
-          v[i].x = (col >= 0 && col < n) ? __ldg(a.x + col) : 0.f;
-          v[i].y = (col + 1 >= 0 && col + 1 < n) ? __ldg(a.x + col + 1) : 0.f;
-          v[i].z = (col + 2 >= 0 && col + 2 < n) ? __ldg(a.x + col + 2) : 0.f;
-          v[i].w = (col + 3 >= 0 && col + 3 < n) ? __ldg(a.x + col + 3) : 0.f;
+        for (int k = 0; k < 5; k++) {
+          const int4 v = __ldg(p + k);
+          d[4 * k] = v.x;
+          d[4 * k + 1] = v.y;
+          d[4 * k + 2] = v.z;
+          d[4 * k + 3] = v.w;
+        }
+      } else {
+#pragma unroll
+        for (int f = 0; f < 20; f++)
+          d[f] = 0;
+      }
+    };
+    // record + elements of tile i into its slot (expected bytes counted; the
+    // slot's phase completes with issue_x's arrival)
+    auto issue_elms = [&](unsigned i) {
+      const int src = (int)(i & 31u);
+      const unsigned e_first = (unsigned)__shfl_sync(0xffffffffu, cl[0], src);
+      const unsigned e_cnt = (unsigned)__shfl_sync(0xffffffffu, cl[1], src);
+      if (lane == 0) {
+        const unsigned slot = i % NS, fb = smem_u32(&full_bar[slot]);
+        const unsigned dst = ring + slot * slot_bytes;
+        const unsigned eb = e_cnt * (unsigned)sizeof(E);
+        mbar_expect_tx(fb, (unsigned)kStageRecBytes + eb);
+        bulk_g2s(dst, recs + (size_t)(t_beg + i) * kStageRecInts, kStageRecBytes, fb);
+        if (eb)
+          bulk_g2s(dst + kStageRecBytes, a.elms + e_first, eb, fb);
+      }
+    };
+    // the tile's x bands: words outside x zero, a ragged end of x by plain
+    // loads (all lanes), then the arrival with the bulk part's bytes
+    auto issue_x = [&](unsigned i) {
+      const int src = (int)(i & 31u);
+      const int nb = __shfl_sync(0xffffffffu, cl[2], src);
+      const unsigned slot = i % NS;
+      float *xs = reinterpret_cast<float *>(smem + slot * slot_bytes + x_off);
+      const int n = (int)a.n_cols;
+      int c0[kStageMaxBands], lo[kStageMaxBands], hi[kStageMaxBands], dst[kStageMaxBands];
+      int d = 0;
+      unsigned xbytes = 0;
+#pragma unroll
+      for (int q = 0; q < kStageMaxBands; q++) {
+        const int c = __shfl_sync(0xffffffffu, cl[4 + 2 * q], src);
+        const int w = __shfl_sync(0xffffffffu, cl[5 + 2 * q], src);
+        c0[q] = c;
+        dst[q] = d;
+        lo[q] = hi[q] = 0;
+        if (q < nb) {
+          // bulk part [lo, hi): inside x, 16-byte chunks
+          const int in_lo = c > 0 ? c : 0;
+          const int in_hi = c + w < n ? c + w : n;
+          lo[q] = in_lo < c + w ? in_lo : c + w;
+          hi[q] = in_hi > lo[q] ? lo[q] + ((in_hi - lo[q]) & ~3) : lo[q];
+          for (int k = c + lane; k < lo[q]; k += 32)
+            xs[d + (k - c)] = 0.f;
+          for (int k = hi[q] + lane; k < c + w; k += 32)
+            xs[d + (k - c)] = k < n ? __ldg(a.x + k) : 0.f;
+          xbytes += (unsigned)(hi[q] - lo[q]) * 4u;
+          d += w;
+        }
+      }
+      __syncwarp();
+      if (lane == 0) {
+        const unsigned fb = smem_u32(&full_bar[slot]);
+        mbar_arrive_expect_tx(fb, xbytes);
+        const unsigned xb = ring + slot * slot_bytes + x_off;
+#pragma unroll
+        for (int q = 0; q < kStageMaxBands; q++)
+          if (q < nb && hi[q] > lo[q])
+            bulk_g2s(xb + 4u * (unsigned)(dst[q] + (lo[q] - c0[q])), a.x + lo[q],
+                     (unsigned)(hi[q] - lo[q]) * 4u, fb);
+      }
+    };
+
+    load_cl(cl, 0);
+    load_cl(nx, 32);
+    const unsigned pre = cnt < NS ? cnt : NS;
+    for (unsigned i = 0; i < pre; i++)
+      issue_elms(i);
+    pdl_wait();
+    if (a.skip && *a.skip) {
+      // the slots' phases complete once the element copies land
+      for (unsigned i = 0; i < pre; i++) {
+        if (lane == 0)
+          mbar_arrive(smem_u32(&full_bar[i]));
+        if (!mbar_wait(smem_u32(&full_bar[i]), 0, nullptr) && lane == 0)
+          atomicCAS(&g_stage_fault, 0u, 3u);
+      }
+      return;
+    }
+    unsigned issued = 0;
+    for (unsigned i = 0; i < cnt; i++) {
+      if (i && (i & 31u) == 0) {
+#pragma unroll
+        for (int f = 0; f < 20; f++)
+          cl[f] = nx[f];
+        load_cl(nx, i + 32);
+      }
+      if (i >= pre) {
+        if (!mbar_wait(smem_u32(&empty_bar[i % NS]), ((i / NS) - 1) & 1u, abort)) {
+          if (lane == 0)
+            stage_fault(2, abort);
+          break;
+        }
+        issue_elms(i);
+      }
+      issue_x(i);
+      issued = i + 1;
+    }
+    if (*abort) {
+      // copies issued into this CTA's shared memory land before it exits
+      const unsigned from = issued > NS ? issued - NS : 0;
+      for (unsigned i = from; i < issued; i++)
+        if (!mbar_wait(smem_u32(&full_bar[i % NS]), (i / NS) & 1u, nullptr) && lane == 0)
+          atomicCAS(&g_stage_fault, 0u, 3u);
+    }
+    pdl_trigger();
+  } else {
+    // ---- consumers -----------------------------------------------------------
+    pdl_wait();
+    if (a.skip && *a.skip)
+      return;
+    for (unsigned i = (unsigned)warp; i < cnt; i += kStageConsumers) {
+      const unsigned slot = i % NS;
+      if (!mbar_wait(smem_u32(&full_bar[slot]), (i / NS) & 1u, abort)) {
+        if (lane == 0)
+          stage_fault(1, abort);
+        break;
+      }
+      const unsigned char *sl = smem + slot * slot_bytes;
+      const int *rc = reinterpret_cast<const int *>(sl);
+      const E *el = reinterpret_cast<const E *>(sl + kStageRecBytes);
+      const float *xs = reinterpret_cast<const float *>(sl + x_off);
+      const unsigned tile = t_beg + i;
+      const int kind = rc[0], nu = rc[1];
+      const unsigned rows = (unsigned)rc[2] * S;
+      const unsigned row0 = tile * kStageTileRows;
+      // rows lane + 32 j; past the tile's last row, read a valid row's
+      // operands (the result is not stored)
+      unsigned tt[8];
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const unsigned t = (unsigned)lane + 32u * j;
+        tt[j] = t < rows ? t : rows - 1;
+      }
+      // epilogue operands from global memory, in flight during the walk
+      float vj[8], dj[8], xj[8];
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        vj[j] = dj[j] = xj[j] = 0.f;
+        if (a.ep.out)
+          vj[j] = static_cast<const float *>(a.ep.v)[row0 + tt[j]];
+        if constexpr (std::is_same<E, __half>::value) {
+          if (a.dg) {
+            dj[j] = __ldcs(a.dg + row0 + tt[j]);
+            xj[j] = ld_x_guard(a.x, row0 + tt[j], a.n_cols);
+          }
+        }
+      }
+      float acc[8];
+#pragma unroll
+      for (int j = 0; j < 8; j++)
+        acc[j] = 0.f;
+      if (kind == 1) {
+        // every slice carries all nu windows: element of (row t, window u)
+        // at (t / S) nu S + u S + t mod S
+        const E *ep[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+          ep[j] = el + (tt[j] / S) * (unsigned)nu * S + (tt[j] & (S - 1));
+        for (int u = 0; u < nu; u++) {
+          const float *xu = xs + rc[8 + u];
+          const unsigned eo = (unsigned)u * S;
+#pragma unroll
+          for (int j = 0; j < 8; j++)
+            acc[j] = fmaf(float(ep[j][eo]), xu[tt[j]], acc[j]);
+        }
+      } else if (kind == 2) {
+        // slices differ: the k-th set bit of the slice's mask is its k-th
+        // diagonal
+        unsigned long long mk[8];
+        const E *ep[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          const unsigned s = tt[j] / S;
+          mk[j] = ((unsigned long long)(unsigned)rc[73 + 2 * s] << 32) | (unsigned)rc[72 + 2 * s];
+          ep[j] = el + rc[104 + s] + (tt[j] & (S - 1));
+        }
+        for (int u = 0; u < nu; u++) {
+          const float *xu = xs + rc[8 + u];
+#pragma unroll
+          for (int j = 0; j < 8; j++)
+            if ((mk[j] >> u) & 1ull) {
+              acc[j] = fmaf(float(*ep[j]), xu[tt[j]], acc[j]);
+              ep[j] += S;
+            }
+        }
+        // entries with explicit columns (kernel.h:70-79): elements staged
+        // before the slice's diagonals, columns and x from global memory
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          const unsigned s = tt[j] / S, r = tt[j] & (S - 1);
+          const int ne = rc[120 + s];
+          const E *ee = el + rc[104 + s] - ne * (int)S + r;
+          const unsigned *cc = a.cols + (unsigned)rc[136 + s] + r;
+          for (int q = 0; q < ne; q++)
+            acc[j] = fmaf(float(ee[q * S]), ld_x_guard(a.x, __ldg(cc + q * S), a.n_cols), acc[j]);
+        }
+      }
+      __syncwarp();
+      if (lane == 0)
+        mbar_arrive(smem_u32(&empty_bar[slot]));
+      if (kind == 0) {
+        // not staged: the slice walk from global memory (kernel.h:70-92)
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          const unsigned t = tt[j];
+          const unsigned b = tile * spt + t / S, r = t & (S - 1);
+          const unsigned *h = a.sp + 3 * (size_t)b;
+          const unsigned e0 = __ldg(h), c0 = __ldg(h + 1), d0 = __ldg(h + 2);
+          const unsigned e1 = __ldg(h + 3), c1 = __ldg(h + 4);
+          float s = 0.f;
+          for (unsigned q = 0; q < c1 - c0; q += S)
+            s = fmaf(float(a.elms[e0 + q + r]), ld_x_guard(a.x, __ldg(a.cols + c0 + q + r), a.n_cols),
+                     s);
+          const unsigned nd = (e1 - e0 - (c1 - c0)) / S;
+          for (unsigned k = 0; k < nd; k++)
+            s = fmaf(float(a.elms[e0 + (c1 - c0) + k * S + r]),
+                     ld_x_guard(a.x, __ldg(a.sp + d0 + k) + r - S, a.n_cols), s);
+          acc[j] = s;
         }
       }
 #pragma unroll
-      for (int i = 0; i < kStageMaxChunks; i++)
-        if (dst[i] >= 0)
-          *reinterpret_cast<float4 *>(xs + dst[i]) = v[i];
-    }
-    __syncthreads();
-    if (kind == 1) {
-      if (act) {
-        group_uniform<0>(rec, 0, rec[28], ep, S, xs4, tid, acc);
-        group_uniform<1>(rec, rec[28], rec[29], ep, S, xs4, tid, acc);
-        group_uniform<2>(rec, rec[29], rec[30], ep, S, xs4, tid, acc);
-        group_uniform<3>(rec, rec[30], rec[31], ep, S, xs4, tid, acc);
-      }
-    } else {
-      const unsigned long long mask =
-          act ? ((unsigned long long)(unsigned)rec[97 + 2 * s] << 32) | (unsigned)rec[96 + 2 * s]
-              : 0ull;
-      group_masked<0>(rec, 0, rec[28], mask, ep, S, xs4, tid, acc);
-      group_masked<1>(rec, rec[28], rec[29], mask, ep, S, xs4, tid, acc);
-      group_masked<2>(rec, rec[29], rec[30], mask, ep, S, xs4, tid, acc);
-      group_masked<3>(rec, rec[30], rec[31], mask, ep, S, xs4, tid, acc);
-    }
-  } else if (act) {
-    // read-only-path walk of the slice (kernel.h:80-92)
-    const unsigned nd = (e1 - e0 - (c1 - c0)) / S;
-    const unsigned d0 = __ldg(h + 2);
-    const unsigned adj = r - S;
-#pragma unroll 2
-    for (unsigned k = 0; k < nd; k++) {
-      const Vec<4, E> e = ld_stream<4>(ep + (size_t)k * S);
-      const unsigned base = __ldg(a.sp + d0 + k) + adj;
-#pragma unroll
-      for (int j = 0; j < 4; j++)
-        acc[j] = fmaf(float(e.v[j]), ld_x_guard(a.x, base + j, a.n_cols), acc[j]);
-    }
-  }
-  // entries off the slice's diagonals, with explicit columns (kernel.h:70-79)
-  const unsigned nell = act ? (c1 - c0) / S : 0u;
-  for (unsigned jj = 0; jj < nell; jj++) {
-    const size_t q = (size_t)jj * S + r;
-    const Vec<4, E> e = ld_stream<4>(a.elms + e0 + q);
-    const Vec<4, unsigned> cc = ld_stream<4>(a.cols + c0 + q);
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-      acc[j] = fmaf(float(e.v[j]), ld_x_guard(a.x, cc.v[j], a.n_cols), acc[j]);
-  }
-
-  pdl_trigger();
-  const unsigned row = tile * kStageTileRows + t0;
-  if constexpr (std::is_same<E, __half>::value) {
-    // FP16 elements: y = inv_scale * (stored sum), plus diag * x for a split
-    if (act) {
-      if (a.dg) {
-        const float4 dg = __ldcs(reinterpret_cast<const float4 *>(a.dg + row));
-        acc[0] = fmaf(dg.x, ld_x_guard(a.x, row, a.n_cols), acc[0] * a.inv_scale);
-        acc[1] = fmaf(dg.y, ld_x_guard(a.x, row + 1, a.n_cols), acc[1] * a.inv_scale);
-        acc[2] = fmaf(dg.z, ld_x_guard(a.x, row + 2, a.n_cols), acc[2] * a.inv_scale);
-        acc[3] = fmaf(dg.w, ld_x_guard(a.x, row + 3, a.n_cols), acc[3] * a.inv_scale);
-      } else {
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-          acc[j] *= a.inv_scale;
+      for (int j = 0; j < 8; j++) {
+        const unsigned t = (unsigned)lane + 32u * j;
+        if (t < rows) {
+          float yv = acc[j];
+          if constexpr (std::is_same<E, __half>::value)
+            yv = a.dg ? fmaf(dj[j], xj[j], yv * a.inv_scale) : yv * a.inv_scale;
+          a.y[row0 + t] = yv;
+          if (a.ep.out) {
+            dv = fma((double)yv, (double)vj[j], dv);
+            if (two)
+              dw = fma((double)vj[j], (double)vj[j], dw);
+          }
+        }
       }
     }
+    pdl_trigger();
   }
-  if (act)
-    *reinterpret_cast<float4 *>(a.y + row) = make_float4(acc[0], acc[1], acc[2], acc[3]);
   if (a.ep.out) {
-    double dv = 0.0, dw = 0.0;
-    const bool two = a.ep.out2 != nullptr;
-    if (act) {
-      const float4 vv =
-          *reinterpret_cast<const float4 *>(static_cast<const float *>(a.ep.v) + row);
-      const float w[4] = {vv.x, vv.y, vv.z, vv.w};
-#pragma unroll
-      for (int j = 0; j < 4; j++) {
-        dv = fma((double)acc[j], (double)w[j], dv);
-        if (two)
-          dw = fma((double)w[j], (double)w[j], dw);
-      }
-    }
     if (two)
       finish_dot2(dv, dw, a.ep);
     else
@@ -250,30 +400,48 @@ __global__ void __launch_bounds__(kStageThreads, 5)
 }
 
 // The staged walk serves this launch: FP32 vectors, diagonal blocks, fixed
-// slice height in [16, 1024] dividing the tile, the shape N = S, H = 1,
-// 16-byte aligned matrix arrays and y, and tile records registered for the
-// matrix.
+// slice height in [16, 256], the shape N = S, H = 1, x 16-byte aligned,
+// tile records registered for the matrix and at least three ring slots
+// within the shared-memory budget.
 bool staged_shape(int x_dtype, const ispm_launch_params &p, const ispm_slell_view &m,
-                  const void *y, StageInfo &si)
+                  const void *x, StageInfo &si, int &slots, int &slot_bytes, int &x_off)
 {
-  return x_dtype == ISPM_F32 && m.diags && !m.var_height && m.hblock == 1 && p.H == 1 &&
-         p.N == m.slice_height && m.slice_height >= 16 &&
-         kStageTileRows % m.slice_height == 0 && aligned(m.elms, 16) &&
-         aligned(m.cols, 16) && aligned(y, 16) && find_stage_records(m.slice_ptr, m.n_slices, si);
+  if (!(x_dtype == ISPM_F32 && m.diags && !m.var_height && m.hblock == 1 && p.H == 1 &&
+        p.N == m.slice_height && m.slice_height >= 16 && kStageTileRows % m.slice_height == 0 &&
+        aligned(x, 16) && find_stage_records(m.slice_ptr, m.n_slices, si)))
+    return false;
+  const long long esz = m.elm_dtype == ISPM_F32 ? 4 : 2;
+  const long long eb = ((long long)si.max_elms * esz + 15) / 16 * 16;
+  const long long bytes = kStageRecBytes + eb + 4ll * si.max_x_words;
+  const long long ns = std::min<long long>(kStageMaxSlots, kStageSmemBudget / bytes);
+  if (ns < 3)
+    return false;
+  slots = (int)ns;
+  slot_bytes = (int)bytes;
+  x_off = (int)(kStageRecBytes + eb);
+  return true;
 }
 
 template <class E>
 int launch_staged(SpmvArgs<float, E> args, const StageInfo &si, cudaStream_t stream)
 {
   const unsigned spt = kStageTileRows / args.slice_height;
-  const unsigned grid = (args.n_slices + spt - 1) / spt;
-  // the largest band footprint over the matrix's tiles, at most 40 KB (with
-  // the static record the CTA stays inside the 48 KB a launch gets without
-  // opting in to more); tiles over it read x directly
-  const size_t smem = std::min<size_t>((size_t)si.max_words * sizeof(float), 40960);
-  args.stage_words = (int)(smem / sizeof(float));
-  cudaError_t e = launch_kernel(slell_spmv_staged_kernel<E>, dim3(grid), dim3(kStageThreads),
-                                smem, stream, args.pdl != 0, args, si.rec);
+  const unsigned n_tiles = (args.n_slices + spt - 1) / spt;
+  const unsigned grid = std::min<unsigned>(n_tiles, (unsigned)device_sm_count());
+  const size_t smem = (size_t)args.st_slots * (size_t)args.st_slot_bytes;
+  // the ring needs the opt-in shared-memory size, set once per device
+  static std::atomic<unsigned long long> opted{0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess && (dev < 0 || dev >= 64 || !((opted.load() >> dev) & 1ull))) {
+    e = cudaFuncSetAttribute(slell_spmv_staged_kernel<E>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, kStageSmemBudget);
+    if (e == cudaSuccess && dev >= 0 && dev < 64)
+      opted.fetch_or(1ull << dev);
+  }
+  if (e == cudaSuccess && grid)
+    e = launch_kernel(slell_spmv_staged_kernel<E>, dim3(grid), dim3(kStageThreads), smem, stream,
+                      args.pdl != 0, args, si.rec);
   if (e == cudaSuccess)
     e = cudaPeekAtLastError();
   if (e != cudaSuccess)

@@ -112,6 +112,7 @@ def _declare(L):
         "ispm_dslell_upload": (i, [vp, C.POINTER(vp)]),
         "ispm_dslell_upload_f16": (i, [vp, C.POINTER(vp)]),
         "ispm_slell_stage_records": (i, [vp, vp, C.c_longlong, C.POINTER(C.c_longlong)]),
+        "ispm_spmv_stage_fault": (i, [C.POINTER(i)]),
         "ispm_dslell_update_elms": (i, [vp, vp]),
         "ispm_dslell_get_view": (i, [vp, C.POINTER(slell_view)]),
         "ispm_dslell_free": (None, [vp]),
@@ -320,13 +321,13 @@ class slell_matrix:
         return device_slell_matrix(out.value, owner=True)
 
     def stage_records(self) -> np.ndarray:
-        """Tile records of the staged SpMV walk (224 ints per 1024-row tile)."""
+        """Tile records of the staged SpMV walk (176 ints per 256-row tile)."""
         L = _lib()
         n = C.c_longlong()
         _check(L.ispm_slell_stage_records(self._h, None, 0, C.byref(n)))
         out = np.zeros(max(n.value, 1), np.int32)
         _check(L.ispm_slell_stage_records(self._h, _ptr(out), n.value, C.byref(n)))
-        return out[: n.value].reshape(-1, 224) if n.value else out[:0].reshape(0, 224)
+        return out[: n.value].reshape(-1, 176) if n.value else out[:0].reshape(0, 176)
 
 
 class device_slell_matrix:
@@ -462,7 +463,8 @@ class device_split_f16:
 def launch_spmv_split(params: spmv_launch_params, view: slell_view, diag, inv_scale: float,
                       x, y, stream=None):
     """y = inv_scale * (A_off x) + diag * x: `view` describes the off-diagonal
-    part with FP16 elements (elm_dtype F16) in device memory."""
+    part with FP16 elements (elm_dtype F16) in device memory; diag None:
+    y = inv_scale * (A x) (an FP16-stored factor)."""
     L = _lib()
     vp = C.c_void_p
     L.ispm_launch_spmv_split.argtypes = [C.POINTER(spmv_launch_params), C.POINTER(slell_view),
@@ -470,6 +472,15 @@ def launch_spmv_split(params: spmv_launch_params, view: slell_view, diag, inv_sc
     L.ispm_launch_spmv_split.restype = C.c_int
     _check(L.ispm_launch_spmv_split(C.byref(params), C.byref(view), _ptr(diag),
                                     float(inv_scale), _ptr(x), _ptr(y), _stream(stream)))
+
+
+def spmv_stage_fault() -> int:
+    """The staged SpMV walk's wait-timeout record since the last call (0:
+    none; 1 a compute warp's wait, 2 the copy warp's wait, 3 its final
+    wait), cleared by the call."""
+    code = C.c_int()
+    _check(_lib().ispm_spmv_stage_fault(C.byref(code)))
+    return code.value
 
 
 # ---------------------------------------------------------------------------

@@ -134,6 +134,13 @@ def test_split_spmv_matches_oracle(ispm, oracle, cuda, gen, mode):
                                                   1, 1, 1))
         elif dv.slice_height <= 64:
             shapes.append(ispm.spmv_launch_params(64, dv.slice_height, 1, 1, 1))
+        if dv.hblock == 1:  # eight rows a thread: one 16-byte element load
+            if dv.var_height and dv.min_slice_height >= 8:
+                n8 = max(dv.max_slice_height // 8, 4)
+                shapes.append(ispm.spmv_launch_params(n8, n8 * 8, 8, 1, 1))
+            elif not dv.var_height and dv.slice_height >= 32:
+                shapes.append(ispm.spmv_launch_params(dv.slice_height // 8, dv.slice_height,
+                                                      8, 1, 1))
         for p in shapes:
             y = torch.full((dv.n_rows + 8,), float("nan"), dtype=torch.float32, device="cuda")
             d.apply(p, xt, y)

@@ -23,11 +23,14 @@ def as_dict(B):
                 slice_ptr=B.slice_ptr, cols=B.cols, elms=B.elms.copy())
 
 
-def launches(B):
+def launches(B, T=None):
+    """Every valid launch shape; H = 8 (eight rows a thread, FP32 vectors and
+    hblock 1 only) is this library's addition to the reference's 1, 2, 4."""
     v = B.view()
     out = []
+    hs = (1, 2, 4, 8) if T == np.float32 and v.hblock == 1 else (1, 2, 4)
     for N in (4, 8, 16, 32, 64, 128, 256, 512, 1024):
-        for H in (1, 2, 4):
+        for H in hs:
             S = N * H if v.var_height else v.slice_height
             if v.var_height and (N * H < v.max_slice_height or H > v.min_slice_height):
                 continue
@@ -53,7 +56,7 @@ def check_case(ispm, oracle, torch, A, mode, T, E, seed=0, all_launches=True):
     rel = REL[(T, E)]
     xt = torch.from_numpy(x.copy()).cuda() if A.n_cols else torch.zeros(1, dtype=torch.float64 if T == np.float64 else torch.float32, device="cuda")
     tdt = torch.float64 if T == np.float64 else torch.float32
-    todo = launches(B) if all_launches else launches(B)[:3]
+    todo = launches(B, T) if all_launches else launches(B)[:3]
     assert todo, "no valid launch shape"
     for N, SS, H in todo:
         y = torch.full((B.n_rows + 8,), float("nan"), dtype=tdt, device="cuda")
@@ -70,6 +73,8 @@ def check_case(ispm, oracle, torch, A, mode, T, E, seed=0, all_launches=True):
         if den > 0:
             assert np.linalg.norm(err) / den <= rel, (mode, N, H)
         # the oracle's emulation of the reference kernel's own summation order
+        if H == 8:
+            continue
         yk = oracle.slell_spmv_kernel_order(m, x, N, H).astype(np.float64)
         if den > 0:
             assert np.linalg.norm(yk - y_ex) / den <= rel

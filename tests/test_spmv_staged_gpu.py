@@ -1,14 +1,17 @@
-"""The x-window staging SpMV (launch shape N = S, H = 1 on diagonal-block
-matrices) against the CPU oracle's long-double slice walk (cuda/spmv/kernel.h:80-92).
+"""The staged SpMV walk (launch shape N = S, H = 1 on diagonal-block
+matrices: 256-row tiles whose elements and x bands a copy warp moves into
+shared memory with bulk copies) against the CPU oracle's long-double slice
+walk (cuda/spmv/kernel.h:80-92).
 
-The staged walk copies each CTA tile's x windows into shared memory when every
-slice of the tile carries the same diagonal offsets and the windows fit the
-staging budget; other tiles read x through the read-only path.  These cases
-drive each branch: uniform interior tiles, boundary tiles whose slices differ,
-bands reaching past either end of x (zero fill), bands over the budget,
-more diagonals than the staged walk takes, rectangular matrices, x whose
-length is not a multiple of four and x not 16-byte aligned (scalar staging),
-every slice height the shape allows, and both vector types.
+Tiles stage when their windows fit 64 diagonals, 8 bands and the x-area
+budget; other tiles read everything from global memory.  These cases drive
+each branch: uniform interior tiles, boundary tiles whose slices differ or
+carry explicit-column entries, bands reaching past either end of x (zero
+fill, a ragged last chunk), bands over the limits, more diagonals than the
+staged walk takes, rectangular matrices, x not 16-byte aligned (the launch
+takes the register walk), every slice height (512 exceeds a tile: register
+walk), both vector types, FP16 split and FP16 factor elements.  After every
+launch the kernel's wait-timeout record must read 0.
 
 Tolerances as in test_spmv_gpu: FP64 within 1e-14, FP32 within 1e-6
 (norm-wise, relative to sum |a_ij x_j|), and every row within
@@ -62,6 +65,7 @@ def run_staged(ispm, oracle, torch, A, S, T, E, x_offset=0):
     y = torch.full((B.n_rows + 8,), float("nan"), dtype=tdt, device="cuda")
     ispm.launch_spmv_kernel(ispm.spmv_launch_params(S, S, 1, 1, 1), dB, xt, y)
     torch.cuda.synchronize()
+    assert ispm.spmv_stage_fault() == 0
     yh = y.cpu().numpy()
     assert np.all(np.isnan(yh[B.n_rows:])), "wrote past the padded rows"
     yh = yh[: B.n_rows].astype(np.float64)
@@ -89,8 +93,8 @@ def test_staged_stencils(ispm, oracle, cuda, gen, S, T, E):
 
 @pytest.mark.parametrize("T,E", TE, ids=["dd", "df", "ff"])
 def test_staged_far_apart_diagonals_exceed_budget(ispm, oracle, cuda, T, E):
-    # 15 diagonals 700 apart: 15 bands of at least 256 words each, beyond the
-    # staging budget of 12 words per tile row -> interior tiles read x directly
+    # 15 diagonals 700 apart: 15 bands, more than the 8 a tile stages ->
+    # interior tiles read everything from global memory
     offs = [700 * k for k in range(-7, 8)]
     A = multidiag(ispm, 20000, 20000, offs, 1)
     run_staged(ispm, oracle, cuda, A, 64, T, E)
@@ -143,8 +147,38 @@ def test_staged_split_operator(ispm, oracle, cuda, gen):
     y = torch.full((dv.n_rows + 8,), float("nan"), dtype=torch.float32, device="cuda")
     d.apply(p, torch.from_numpy(x).cuda(), y)
     torch.cuda.synchronize()
+    assert ispm.spmv_stage_fault() == 0
     yh = y.cpu().numpy()
     assert np.all(np.isnan(yh[dv.n_rows:]))
     err = np.abs(yh[: dv.n_rows].astype(np.float64) - y_ex)
     assert np.all(err <= gamma * absrow + 1e-300), err.max()
     assert np.linalg.norm(err) / np.linalg.norm(absrow) <= 1e-6
+
+
+@pytest.mark.parametrize("S", [32, 64])
+def test_staged_f16_factor(ispm, oracle, cuda, gen, S):
+    """FP16-stored elements times a power of two without a diagonal vector
+    (the factor_f16 option's G and G^T): y = inv_scale * (stored sum)."""
+    torch = cuda
+    A = gen.stencil_grf(40, 27, 8.0, 1.5, 3)
+    ge = A.elms.astype(np.float64)
+    e = int(np.floor(np.log2(np.abs(ge).max())))
+    sc = 2.0 ** (14 - e)
+    v16 = (ge * sc).astype(np.float16).astype(np.float32)
+    H = ispm.csr_to_slell(ispm.csr_matrix(A.n_rows, A.n_cols, A.row_ptr, A.cols, v16), S, 1, 0, 1)
+    dH = H.upload_f16()
+    x = np.random.default_rng(9).uniform(-1, 1, A.n_cols).astype(np.float32)
+    y_st, ab_st = oracle.slell_spmv_exact(as_dict(H), x)
+    y_ex, absrow = y_st / sc, ab_st / sc
+    k = int(np.diff(A.row_ptr).max()) + 1
+    gamma = k * 2.0 ** -24 / (1 - k * 2.0 ** -24)
+    for p in (ispm.spmv_launch_params(S, S, 1, 1, 1), ispm.default_launch_params(dH.view(), ispm.F32)):
+        y = torch.full((H.n_rows + 8,), float("nan"), dtype=torch.float32, device="cuda")
+        ispm.launch_spmv_split(p, dH.view(), None, 1.0 / sc, torch.from_numpy(x).cuda(), y)
+        torch.cuda.synchronize()
+        assert ispm.spmv_stage_fault() == 0
+        yh = y.cpu().numpy()
+        assert np.all(np.isnan(yh[H.n_rows:]))
+        err = np.abs(yh[: H.n_rows].astype(np.float64) - y_ex)
+        assert np.all(err <= gamma * absrow + 1e-300), (p.N, p.H, err.max())
+        assert np.linalg.norm(err) / np.linalg.norm(absrow) <= 1e-6
