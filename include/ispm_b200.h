@@ -137,8 +137,8 @@ int ispm_dslell_upload_f16(const ispm_slell *h, ispm_dslell **out);
 int ispm_slell_stage_records(const ispm_slell *m, int *out, long long cap, long long *n_ints);
 /* The staged walk's wait-timeout record: *code = 0, or the first timeout a
  * staged launch met since the last call (1 a consumer warp's wait for a
- * tile, 2 the copy warp's wait for a free slot, 3 the final wait for its
- * copies); the record is cleared.  Synchronous. */
+ * tile, 2 the copy warp's wait for a free slot); the record is cleared.
+ * Synchronous. */
 int ispm_spmv_stage_fault(int *code);
 /* Re-upload only the element values of a matrix with unchanged structure
  * (plan/plan.h:39-42, implemented as the element-only H2D copy it means). */

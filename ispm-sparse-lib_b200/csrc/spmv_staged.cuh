@@ -4,34 +4,38 @@
 //
 // In the reference walk (cuda/spmv/kernel.h:80-92) the thread of local row r
 // reads x[diag_pos + r - S] for every diagonal of its slice, two dependent
-// loads per element on the critical path.  Here the GPU's copy engine feeds
-// the FMAs: a persistent CTA per SM takes a contiguous run of 256-row tiles;
-// one producer warp moves each tile's record, its elements (one contiguous
-// range: staged tiles have diagonal blocks only) and the bands of x its
-// windows read (zero outside x) into a ring of shared-memory slots with bulk
-// asynchronous copies (cp.async.bulk) completing on an mbarrier per slot;
-// four consumer warps take the tiles in turn, each lane eight rows (t = lane
-// + 32 j), reading every element and x value from shared memory with
-// conflict-free 32-bit loads, and hand the slot back through a second
-// mbarrier.  The element copies of the first slots go out before the
-// programmatic-launch wait (the matrix is final before the previous kernel
-// starts), the x copies after it.  The producer keeps up to `slots` tiles in
-// flight, so the bytes in flight per SM are set by shared memory, not by
-// registers or warps.
+// loads per element on the critical path.  Here asynchronous copies feed the
+// FMAs: a persistent CTA per SM takes a contiguous run of 256-row tiles;
+// copy warps move each tile's record, its elements (one contiguous range: a
+// tile's slices are consecutive in elms) and the bands of x its windows read
+// (zero outside x) into a ring of shared-memory slots with 16-byte cp.async
+// copies, each copy lane's copies completing on the slot's mbarrier
+// (cp.async.mbarrier.arrive.noinc); compute warps take the tiles in turn,
+// each lane eight rows (t = lane + 32 j), reading every element and x value
+// from shared memory with conflict-free 32-bit loads, and hand the slot back
+// through a second mbarrier.  The element copies of the first slots go out
+// before the programmatic-launch wait (the matrix is final before the
+// previous kernel starts), the x copies after it.  The copy warps keep up to
+// `slots` tiles in flight, so the bytes in flight per SM are set by shared
+// memory, not by registers or warps.  (Measured on this walk: the bulk-copy
+// engine, cp.async.bulk, moves about 17 bytes per cycle per SM, and one
+// warp's 16-byte lane copies about 7, against the 25 an SM's share of HBM
+// needs; hence several copy warps.)
 //
 // Every wait on an mbarrier is bounded (about 2^31 clock cycles): on a
-// timeout the CTA records a fault code in g_stage_fault, stops issuing and
-// waiting, and the producer waits (bounded) for the copies it issued before
-// the CTA exits.  The host reads and clears the code with
-// ispm_spmv_stage_fault().
+// timeout the CTA records a fault code in g_stage_fault and stops issuing
+// and waiting; the copy lanes wait for their own copies before the CTA
+// exits.  The host reads and clears the code with ispm_spmv_stage_fault().
 
 constexpr int kStageConsumers = 4;                     // compute warps
-constexpr int kStageThreads = 32 * (kStageConsumers + 1);
+constexpr int kStageProducers = 4;                     // copy warps
+constexpr int kStageThreads = 32 * (kStageConsumers + kStageProducers);
+constexpr unsigned kStageCopyLanes = 32u * kStageProducers;
 constexpr int kStageMaxSlots = 8;
 constexpr int kStageSmemBudget = 220 * 1024;           // dynamic shared memory for the ring
 constexpr int kStageRecBytes = kStageRecComputeInts * 4;
 
-__device__ unsigned g_stage_fault;  // 0, or the first timeout's code (1 consumer, 2 producer, 3 drain)
+__device__ unsigned g_stage_fault;  // 0, or the first timeout's code (1 consumer, 2 producer)
 
 __device__ __forceinline__ unsigned smem_u32(const void *p)
 {
@@ -40,17 +44,6 @@ __device__ __forceinline__ unsigned smem_u32(const void *p)
 __device__ __forceinline__ void mbar_init(unsigned b, unsigned count)
 {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(b), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned b, unsigned bytes)
-{
-  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(b), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned b, unsigned bytes)
-{
-  asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(b),
-               "r"(bytes)
-               : "memory");
 }
 __device__ __forceinline__ void mbar_arrive(unsigned b)
 {
@@ -82,16 +75,21 @@ __device__ __forceinline__ bool mbar_wait(unsigned b, unsigned parity, const vol
       return false;
   }
 }
-// Global -> shared bulk copy completing `bytes` on barrier b (16-byte
-// aligned addresses, bytes a multiple of 16).
-__device__ __forceinline__ void bulk_g2s(unsigned dst, const void *src, unsigned bytes, unsigned b)
+// 16-byte global -> shared copy (16-byte aligned addresses); the bytes past
+// the first src_bytes (0..16) are zero and not read.
+__device__ __forceinline__ void cp16(unsigned dst, const void *src, unsigned src_bytes)
 {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-          "r"(dst),
-      "l"(src), "r"(bytes), "r"(b)
-      : "memory");
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src),
+               "r"(src_bytes)
+               : "memory");
 }
+// One arrival on barrier b once every earlier cp.async of this thread has
+// landed (the barrier's count includes it).
+__device__ __forceinline__ void cp_arrive(unsigned b)
+{
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(b) : "memory");
+}
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 __device__ __forceinline__ void stage_fault(unsigned code, volatile int *abort)
 {
@@ -120,8 +118,8 @@ __global__ void __launch_bounds__(kStageThreads, 1)
   const unsigned ring = smem_u32(smem);
   if (threadIdx.x == 0) {
     for (unsigned s = 0; s < NS; s++) {
-      mbar_init(smem_u32(&full_bar[s]), 1);
-      mbar_init(smem_u32(&empty_bar[s]), 1);
+      mbar_init(smem_u32(&full_bar[s]), kStageCopyLanes);  // the copy warps' lanes
+      mbar_init(smem_u32(&empty_bar[s]), 1);  // the consuming warp
     }
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -130,10 +128,12 @@ __global__ void __launch_bounds__(kStageThreads, 1)
 
   double dv = 0.0, dw = 0.0;
   const bool two = a.ep.out2 != nullptr;
-  if (warp == kStageConsumers) {
-    // ---- producer ----------------------------------------------------------
-    // copy lists: lane l holds the one of tile (batch base + l); this batch
-    // in cl, the next one in nx
+  if (warp >= kStageConsumers) {
+    // ---- copy warps ----------------------------------------------------------
+    // copy lane c (of kStageCopyLanes) moves 16-byte chunks c, c + lanes, ...
+    const unsigned cpl = 32u * (unsigned)(warp - kStageConsumers) + (unsigned)lane;
+    // copy lists: lane l of every copy warp holds the one of tile (batch base
+    // + l); this batch in cl, the next one in nx
     int cl[20], nx[20];
     auto load_cl = [&](int(&d)[20], unsigned base) {
       const unsigned tl = t_beg + base + (unsigned)lane;
@@ -154,65 +154,43 @@ __global__ void __launch_bounds__(kStageThreads, 1)
           d[f] = 0;
       }
     };
-    // record + elements of tile i into its slot (expected bytes counted; the
-    // slot's phase completes with issue_x's arrival)
+    // record + elements of tile i into its slot, 16 bytes a lane and step
     auto issue_elms = [&](unsigned i) {
       const int src = (int)(i & 31u);
       const unsigned e_first = (unsigned)__shfl_sync(0xffffffffu, cl[0], src);
       const unsigned e_cnt = (unsigned)__shfl_sync(0xffffffffu, cl[1], src);
-      if (lane == 0) {
-        const unsigned slot = i % NS, fb = smem_u32(&full_bar[slot]);
-        const unsigned dst = ring + slot * slot_bytes;
-        const unsigned eb = e_cnt * (unsigned)sizeof(E);
-        mbar_expect_tx(fb, (unsigned)kStageRecBytes + eb);
-        bulk_g2s(dst, recs + (size_t)(t_beg + i) * kStageRecInts, kStageRecBytes, fb);
-        if (eb)
-          bulk_g2s(dst + kStageRecBytes, a.elms + e_first, eb, fb);
-      }
+      const unsigned dst = ring + (i % NS) * slot_bytes;
+      const char *rs = reinterpret_cast<const char *>(recs + (size_t)(t_beg + i) * kStageRecInts);
+      for (unsigned o = 16u * cpl; o < (unsigned)kStageRecBytes; o += 16u * kStageCopyLanes)
+        cp16(dst + o, rs + o, 16);
+      const char *es = reinterpret_cast<const char *>(a.elms + e_first);
+      const unsigned eb = e_cnt * (unsigned)sizeof(E);
+      for (unsigned o = 16u * cpl; o < eb; o += 16u * kStageCopyLanes)
+        cp16(dst + kStageRecBytes + o, es + o, 16);
     };
-    // the tile's x bands: words outside x zero, a ragged end of x by plain
-    // loads (all lanes), then the arrival with the bulk part's bytes
+    // the tile's x bands (columns outside x read zero), then each lane's
+    // arrival on the slot once its copies of the tile have landed
     auto issue_x = [&](unsigned i) {
       const int src = (int)(i & 31u);
       const int nb = __shfl_sync(0xffffffffu, cl[2], src);
       const unsigned slot = i % NS;
-      float *xs = reinterpret_cast<float *>(smem + slot * slot_bytes + x_off);
+      const unsigned xb = ring + slot * slot_bytes + x_off;
       const int n = (int)a.n_cols;
-      int c0[kStageMaxBands], lo[kStageMaxBands], hi[kStageMaxBands], dst[kStageMaxBands];
       int d = 0;
-      unsigned xbytes = 0;
 #pragma unroll
       for (int q = 0; q < kStageMaxBands; q++) {
         const int c = __shfl_sync(0xffffffffu, cl[4 + 2 * q], src);
         const int w = __shfl_sync(0xffffffffu, cl[5 + 2 * q], src);
-        c0[q] = c;
-        dst[q] = d;
-        lo[q] = hi[q] = 0;
         if (q < nb) {
-          // bulk part [lo, hi): inside x, 16-byte chunks
-          const int in_lo = c > 0 ? c : 0;
-          const int in_hi = c + w < n ? c + w : n;
-          lo[q] = in_lo < c + w ? in_lo : c + w;
-          hi[q] = in_hi > lo[q] ? lo[q] + ((in_hi - lo[q]) & ~3) : lo[q];
-          for (int k = c + lane; k < lo[q]; k += 32)
-            xs[d + (k - c)] = 0.f;
-          for (int k = hi[q] + lane; k < c + w; k += 32)
-            xs[d + (k - c)] = k < n ? __ldg(a.x + k) : 0.f;
-          xbytes += (unsigned)(hi[q] - lo[q]) * 4u;
+          for (int k = 4 * (int)cpl; k < w; k += 4 * (int)kStageCopyLanes) {
+            const int col = c + k;  // a multiple of 4: no chunk straddles column 0
+            const int valid = (col < 0 || col >= n) ? 0 : (n - col >= 4 ? 4 : n - col);
+            cp16(xb + 4u * (unsigned)(d + k), a.x + (valid ? col : 0), 4u * (unsigned)valid);
+          }
           d += w;
         }
       }
-      __syncwarp();
-      if (lane == 0) {
-        const unsigned fb = smem_u32(&full_bar[slot]);
-        mbar_arrive_expect_tx(fb, xbytes);
-        const unsigned xb = ring + slot * slot_bytes + x_off;
-#pragma unroll
-        for (int q = 0; q < kStageMaxBands; q++)
-          if (q < nb && hi[q] > lo[q])
-            bulk_g2s(xb + 4u * (unsigned)(dst[q] + (lo[q] - c0[q])), a.x + lo[q],
-                     (unsigned)(hi[q] - lo[q]) * 4u, fb);
-      }
+      cp_arrive(smem_u32(&full_bar[slot]));
     };
 
     load_cl(cl, 0);
@@ -222,16 +200,9 @@ __global__ void __launch_bounds__(kStageThreads, 1)
       issue_elms(i);
     pdl_wait();
     if (a.skip && *a.skip) {
-      // the slots' phases complete once the element copies land
-      for (unsigned i = 0; i < pre; i++) {
-        if (lane == 0)
-          mbar_arrive(smem_u32(&full_bar[i]));
-        if (!mbar_wait(smem_u32(&full_bar[i]), 0, nullptr) && lane == 0)
-          atomicCAS(&g_stage_fault, 0u, 3u);
-      }
+      cp_wait_all();  // no copy into this CTA's shared memory outlives it
       return;
     }
-    unsigned issued = 0;
     for (unsigned i = 0; i < cnt; i++) {
       if (i && (i & 31u) == 0) {
 #pragma unroll
@@ -248,15 +219,8 @@ __global__ void __launch_bounds__(kStageThreads, 1)
         issue_elms(i);
       }
       issue_x(i);
-      issued = i + 1;
     }
-    if (*abort) {
-      // copies issued into this CTA's shared memory land before it exits
-      const unsigned from = issued > NS ? issued - NS : 0;
-      for (unsigned i = from; i < issued; i++)
-        if (!mbar_wait(smem_u32(&full_bar[i % NS]), (i / NS) & 1u, nullptr) && lane == 0)
-          atomicCAS(&g_stage_fault, 0u, 3u);
-    }
+    cp_wait_all();
     pdl_trigger();
   } else {
     // ---- consumers -----------------------------------------------------------

@@ -476,8 +476,8 @@ def launch_spmv_split(params: spmv_launch_params, view: slell_view, diag, inv_sc
 
 def spmv_stage_fault() -> int:
     """The staged SpMV walk's wait-timeout record since the last call (0:
-    none; 1 a compute warp's wait, 2 the copy warp's wait, 3 its final
-    wait), cleared by the call."""
+    none; 1 a compute warp's wait, 2 the copy warp's wait), cleared by the
+    call."""
     code = C.c_int()
     _check(_lib().ispm_spmv_stage_fault(C.byref(code)))
     return code.value
