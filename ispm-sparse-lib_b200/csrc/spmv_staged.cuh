@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(kStageThreads, 1)
     const unsigned cpl = 32u * (unsigned)(warp - kStageConsumers) + (unsigned)lane;
     // copy lists: lane l of every copy warp holds the one of tile (batch base
     // + l); this batch in cl, the next one in nx
-    int cl[20], nx[20];
+    int cl[20] = {}, nx[20] = {};
     auto load_cl = [&](int(&d)[20], unsigned base) {
       const unsigned tl = t_beg + base + (unsigned)lane;
       if (tl < t_end) {
