@@ -2,6 +2,7 @@
 peak, each timed alone with CUDA events on inputs larger than the 126 MB L2.
 
   python -m ispm.roofline [--json PATH] [--reps K] [--warm W]
+  python -m ispm.roofline --shapes [--json PATH]
 
 For every kernel: its algorithmic bytes per launch (compulsory reads and
 writes, no re-reads), the mean launch time after warm-up, achieved GB/s and
@@ -9,6 +10,12 @@ the fraction of the peak (MEASURED_PEAKS.json's copy bandwidth when present,
 else 6,650 GB/s).  The MLP rows also give tensor-core TFLOP/s against the
 measured BF16 peak.  Sizes: the 128^3 27-point system of the headline
 workload for the matrix kernels, 2^26-element vectors for the BLAS.
+
+--shapes times the SpMV of the headline solver's operators (A in FP32 and
+as the FP16 split, the GPU FSAI factor G and G^T in FP32 and FP16) under
+several launch shapes: the default register walk (N = S/4, H = 4), two and
+eight rows a thread, and the staged walk (N = S, H = 1), back to back
+("warm") and with a 256 MB L2 flush before every launch ("flushed").
 """
 from __future__ import annotations
 
@@ -157,16 +164,98 @@ def run(log=print):
     return {"peak_hbm_gbs": hbm, "peak_bf16_tflops": bf16, "peak_source": src, "rows": rows}
 
 
+def run_shapes(log=print):
+    import torch
+    from . import (gen, ispm_initialize, csr_to_slell, device_split_f16, launch_spmv_split,
+                   spmv_launch_params, spmv_stage_fault)
+    torch.cuda.init()
+    ispm_initialize()
+    hbm, _, src = peaks()
+    dev = torch.device("cuda")
+    flush = torch.empty(1 << 26, dtype=torch.float32, device=dev)  # 256 MB > L2
+    rows = []
+
+    def timed_flushed(fn, n=10):
+        ts = []
+        for _ in range(n):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1) * 1e-3)
+        return float(np.median(ts))
+
+    def shapes_of(name, view, nbytes, apply, shapes):
+        x = torch.rand(view.n_cols, device=dev)
+        y = torch.zeros(view.n_rows, device=dev)
+        for N, H in shapes:
+            p = spmv_launch_params(N, view.slice_height, H, 1, 1)
+            f = lambda: apply(p, x, y)
+            warm, cold = timed(f), timed_flushed(f)
+            r = {"operator": name, "N": N, "S": view.slice_height, "H": H, "bytes": int(nbytes),
+                 "us": warm * 1e6, "frac": nbytes / warm / 1e9 / hbm,
+                 "us_flushed": cold * 1e6, "frac_flushed": nbytes / cold / 1e9 / hbm}
+            rows.append(r)
+            log(f"{name:14s} N={N:3d} S={view.slice_height} H={H}: {r['us']:7.2f} us "
+                f"{r['frac']:.3f} | flushed {r['us_flushed']:7.2f} us {r['frac_flushed']:.3f}")
+        if spmv_stage_fault():
+            raise RuntimeError("the staged walk recorded a wait timeout")
+
+    def nbytes_of(view, esz, extra=0):
+        return (4 * view.n_slice_ptr + 4 * view.n_cols_arr + esz * view.n_nz +
+                4 * (view.n_cols + view.n_rows) + extra)
+
+    A = gen.stencil_grf(128, 27, 8.0, 1.5, 0)
+    n = A.n_rows
+    A32 = csr_matrix(n, n, A.row_ptr, A.cols, A.elms.astype(np.float32))
+    H = csr_to_slell_guess_format(A32)
+    D = H.upload()
+    S = D.view().slice_height
+    regw = [(S // 4, 4), (S // 2, 2), (S // 8, 8), (S, 1)]
+    shapes_of("A FP32", D.view(), nbytes_of(D.view(), 4),
+              lambda p, x, y: launch_spmv_kernel(p, D, x, y), regw)
+    del D, H
+    sp = device_split_f16(A)
+    v = sp.view()
+    shapes_of("A FP16 split", v, nbytes_of(v, 2, 4 * v.n_rows), sp.apply, regw)
+    del sp
+    G1, G2 = fsai_sym_gpu(A, np.float64)
+    for nm, G in (("G", G1), ("G^T", G2)):
+        F = csr_matrix(G.n_rows, G.n_cols, G.row_ptr, G.cols, np.asarray(G.elms).astype(np.float32))
+        Hf = csr_to_slell(F, 64, 1, 0, 1)
+        Df = Hf.upload()
+        shapes_of(nm + " FP32", Df.view(), nbytes_of(Df.view(), 4),
+                  lambda p, x, y: launch_spmv_kernel(p, Df, x, y), [(16, 4), (32, 2), (8, 8), (64, 1)])
+        del Df, Hf
+        # FP16 factor: values times a power of two, the product scaled back
+        ge = np.asarray(G.elms, np.float64)
+        sc = 2.0 ** (14 - int(np.floor(np.log2(np.abs(ge).max()))))
+        v16 = (ge * sc).astype(np.float16).astype(np.float32)
+        Hh = csr_to_slell(csr_matrix(G.n_rows, G.n_cols, G.row_ptr, G.cols, v16), 64, 1, 0, 1)
+        Dh = Hh.upload_f16()
+        vh = Dh.view()
+        shapes_of(nm + " FP16", vh, nbytes_of(vh, 2),
+                  lambda p, x, y: launch_spmv_split(p, vh, None, 1.0 / sc, x, y),
+                  [(16, 4), (8, 8), (64, 1)])
+        del Dh, Hh
+    return {"peak_hbm_gbs": hbm, "peak_source": src, "shapes": rows}
+
+
 def main(argv=None):
     import argparse
     ap = argparse.ArgumentParser(prog="python -m ispm.roofline")
     ap.add_argument("--json", default=None)
     ap.add_argument("--reps", type=int, default=20, help="timed launches per kernel")
     ap.add_argument("--warm", type=int, default=3, help="untimed launches per kernel")
+    ap.add_argument("--shapes", action="store_true",
+                    help="compare SpMV launch shapes on the headline solver's operators")
     a = ap.parse_args(argv)
     global REPS, WARM
     REPS, WARM = max(1, a.reps), max(0, a.warm)
-    out = run(log=lambda *m: print(*m, file=sys.stderr, flush=True))
+    log = lambda *m: print(*m, file=sys.stderr, flush=True)
+    out = run_shapes(log=log) if a.shapes else run(log=log)
     if a.json:
         json.dump(out, open(a.json, "w"), indent=1)
     print(json.dumps(out))
