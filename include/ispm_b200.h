@@ -400,6 +400,13 @@ typedef struct {
                            11 mantissa bits where BF16 keeps 8; half the bytes
                            of each factor application.  Takes precedence over
                            factor_bf16. */
+  int refresh;          /* keep what ispm_solver_update_values needs to take new
+                           values of A (same sparsity pattern) on the device:
+                           the CSR-entry -> element-slot maps of both device
+                           copies of A, the renumbering's entry map and, with
+                           prec = ISPM_PREC_FSAI_GPU, the factor's device
+                           patterns (about 20 bytes per entry of A and 32 per
+                           entry of G).  Not with matrix_f16. */
 } ispm_solver_opts;
 
 #define ISPM_REORDER_NONE 0
@@ -425,7 +432,7 @@ typedef struct {
 /* Defaults: FP32 inner with FP64 reliable updates, tol 1e-10, max_iters
  * 100000, max_refinements 500, check_every 16, use_graph 1,
  * replace_ratio_f32 1e-2, replace_ratio_f64 1e-4, variant AUTO, prec GIVEN,
- * factor_bf16 0, reorder AUTO. */
+ * factor_bf16 0, reorder AUTO, matrix_f16 0, factor_f16 0, refresh 0. */
 void ispm_solver_default_opts(ispm_solver_opts *opts);
 
 typedef struct ispm_solver ispm_solver;
@@ -447,6 +454,18 @@ int ispm_solver_solve(ispm_solver *s, const double *b, double *x, ispm_solve_sta
 /* Same with host vectors of n entries: copies b in and x out inside the call. */
 int ispm_solver_solve_host(ispm_solver *s, const double *b_host, double *x_host,
                            ispm_solve_stats *stats, void *stream);
+/* New values of A for a solver created with opts.refresh = 1: vals holds
+ * row_ptr[n] FP64 values in the CSR order (and sparsity pattern) passed to
+ * ispm_solver_create, on the device when vals_on_device is nonzero, else on
+ * the host.  Both device copies of A are rewritten in place and, with prec =
+ * ISPM_PREC_FSAI_GPU, the FSAI factor pair is rebuilt on the device from the
+ * new values; no conversion, ordering or pattern work runs on the host, so a
+ * time-stepping caller whose matrix keeps its pattern pays this instead of
+ * a new ispm_solver_create.  A given factor pair (prec = ISPM_PREC_GIVEN)
+ * stays as it was.  The values are not checked (a non-SPD matrix shows as a
+ * breakdown in the next solve).  Synchronous.  (The reference's
+ * counterpart for one matrix is spmv_plan::refresh_values, plan/plan.h:39-56.) */
+int ispm_solver_update_values(ispm_solver *s, const double *vals, int vals_on_device);
 /* True relative residual after each outer cycle of the last solve; returns
  * the count (writes at most cap values). */
 int ispm_solver_history(const ispm_solver *s, double *out, int cap);

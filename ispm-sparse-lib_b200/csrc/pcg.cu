@@ -558,6 +558,23 @@ struct Solver {
   // reordered solves: perm[new] = old, and b / x in the solver's order
   int *perm = nullptr;
   double *b_perm = nullptr, *x_perm = nullptr;
+  // opts.refresh: what ispm_solver_update_values needs.  pos_*: CSR entry
+  // (solver order) -> element slot of each device copy of A; entry_src: for
+  // a renumbered solve, solver-order entry -> caller-order entry; a_v: A's
+  // values in solver order (device); fsai: the factor build's device arrays.
+  bool refreshable = false;
+  long long nnz_a = 0;
+  unsigned *pos_ain = nullptr, *pos_a64 = nullptr;
+  int *entry_src = nullptr;
+  double *a_v = nullptr, *a_raw = nullptr;
+  struct FsaiArrays {
+    int *a_rp = nullptr, *a_ci = nullptr, *g_rp = nullptr;
+    unsigned *t_of = nullptr, *pos_g = nullptr, *pos_t = nullptr, *fb = nullptr;
+    double *g_v = nullptr, *gt_v = nullptr;
+    long long nnz_g = 0;
+    bool f16 = false;
+  } fsai;
+  bool fsai_kept = false;
   void *vec[11] = {};
   enum { R, U, W, M, NV, P, S, Q, Z, D, TT };
   cudaGraphExec_t graph = nullptr;
@@ -954,10 +971,48 @@ template <class T> int to_device(DevMem &mem, T **d, const T *h, size_t count)
   return ISPM_OK;
 }
 
+// FSAI values of G from A's device values a_v (solver order, the pattern of
+// f.a_rp / f.a_ci), G^T's by the scatter, both written into the device
+// factor matrices through their CSR-entry -> slot maps (legacy stream).
+int fsai_values(Solver &S, const Solver::FsaiArrays &f, const double *a_v)
+{
+  if (int e = fsai_build_values(S.n, f.a_rp, f.a_ci, a_v, f.g_rp, f.g_v, f.fb, 0))
+    return e;
+  const int blocks = grid_for(f.nnz_g);
+  scatter_kernel<<<blocks, kThreads>>>(f.gt_v, f.t_of, f.g_v, f.nnz_g);
+  ISPM_CUDA_TRY(cudaPeekAtLastError());
+  if (f.f16) {
+    // one power-of-two scale for both factors: the largest magnitude lands
+    // in [2^13, 2^14), below the binary16 maximum (65504)
+    double amax = 0.0;
+    if (int e = device_absmax(f.g_v, f.nnz_g, amax))
+      return e;
+    int ex = 0;
+    if (amax > 0.0)
+      std::frexp(amax, &ex);
+    const double sc = std::ldexp(1.0, amax > 0.0 ? 14 - ex : 0);
+    if (!(sc > 0.0) || !std::isfinite(sc) || sc > 0x1p126 || sc < 0x1p-126)
+      return fail(ISPM_ERR_INVALID, "FP16 factor: magnitudes out of the FP32 scale range");
+    if (int e = refresh_values_f16(S.G.dev, f.pos_g, f.g_v, f.nnz_g, sc, 0))
+      return e;
+    if (int e = refresh_values_f16(S.Ht.dev, f.pos_t, f.gt_v, f.nnz_g, sc, 0))
+      return e;
+    S.G.inv_scale = S.Ht.inv_scale = (float)(1.0 / sc);
+  } else {
+    if (int e = refresh_values(S.G.dev, f.pos_g, f.g_v, ISPM_F64, f.nnz_g, 0))
+      return e;
+    if (int e = refresh_values(S.Ht.dev, f.pos_t, f.gt_v, ISPM_F64, f.nnz_g, 0))
+      return e;
+  }
+  ISPM_CUDA_TRY(cudaMemcpy(&S.fsai_fallbacks, f.fb, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  return ISPM_OK;
+}
+
 // The preconditioner pair from a GPU FSAI build: G on A's lower pattern and
 // its transpose, each stored in its own sliced-ELL shape; the values are
 // computed on the device and scattered into the device matrices through the
-// CSR-entry -> slot maps, so no factor value crosses the host.
+// CSR-entry -> slot maps, so no factor value crosses the host.  With
+// S.refreshable the device arrays stay (S.mem, S.fsai) for value updates.
 int build_fsai_on_device(Solver &S, int n, const int *rp, const int *ci, const double *v)
 {
   std::vector<int> g_rp, g_ci, t_rp, t_ci;
@@ -976,58 +1031,84 @@ int build_fsai_on_device(Solver &S, int n, const int *rp, const int *ci, const d
                           &pos_t, false, bf16, f16))
     return e;
   DevMem tmp;
-  int *a_rp_d, *a_ci_d, *g_rp_d;
-  double *a_v_d, *g_v_d, *gt_v_d;
-  unsigned *t_of_d, *pos_g_d, *pos_t_d, *fb_d;
-  if (int e = to_device(tmp, &a_rp_d, rp, (size_t)n + 1))
+  DevMem &mem = S.refreshable ? S.mem : tmp;
+  Solver::FsaiArrays f;
+  f.nnz_g = (long long)nnz_g;
+  f.f16 = f16;
+  double *a_v_d;
+  if (int e = to_device(mem, &f.a_rp, rp, (size_t)n + 1))
     return e;
-  if (int e = to_device(tmp, &a_ci_d, ci, nnz_a))
+  if (int e = to_device(mem, &f.a_ci, ci, nnz_a))
     return e;
-  if (int e = to_device(tmp, &a_v_d, v, nnz_a))
+  if (S.refreshable && S.a_v) {
+    a_v_d = S.a_v;  // the solver-order values already on the device
+    ISPM_CUDA_TRY(cudaMemcpy(a_v_d, v, nnz_a * sizeof(double), cudaMemcpyHostToDevice));
+  } else if (int e = to_device(mem, &a_v_d, v, nnz_a)) {
     return e;
-  if (int e = to_device(tmp, &g_rp_d, g_rp.data(), g_rp.size()))
-    return e;
-  if (int e = to_device(tmp, &t_of_d, t_of.data(), nnz_g))
-    return e;
-  if (int e = to_device(tmp, &pos_g_d, pos_g.data(), nnz_g))
-    return e;
-  if (int e = to_device(tmp, &pos_t_d, pos_t.data(), nnz_g))
-    return e;
-  if (int e = tmp.get(&g_v_d, nnz_g))
-    return e;
-  if (int e = tmp.get(&gt_v_d, nnz_g))
-    return e;
-  if (int e = tmp.get(&fb_d, 1))
-    return e;
-  if (int e = fsai_build_values(n, a_rp_d, a_ci_d, a_v_d, g_rp_d, g_v_d, fb_d, 0))
-    return e;
-  const int blocks = grid_for((long long)nnz_g);
-  scatter_kernel<<<blocks, kThreads>>>(gt_v_d, t_of_d, g_v_d, (long long)nnz_g);
-  ISPM_CUDA_TRY(cudaPeekAtLastError());
-  if (f16) {
-    // one power-of-two scale for both factors: the largest magnitude lands
-    // in [2^13, 2^14), below the binary16 maximum (65504)
-    double amax = 0.0;
-    if (int e = device_absmax(g_v_d, (long long)nnz_g, amax))
-      return e;
-    int ex = 0;
-    if (amax > 0.0)
-      std::frexp(amax, &ex);
-    const double sc = std::ldexp(1.0, amax > 0.0 ? 14 - ex : 0);
-    if (!(sc > 0.0) || !std::isfinite(sc) || sc > 0x1p126 || sc < 0x1p-126)
-      return fail(ISPM_ERR_INVALID, "FP16 factor: magnitudes out of the FP32 scale range");
-    if (int e = refresh_values_f16(S.G.dev, pos_g_d, g_v_d, (long long)nnz_g, sc, 0))
-      return e;
-    if (int e = refresh_values_f16(S.Ht.dev, pos_t_d, gt_v_d, (long long)nnz_g, sc, 0))
-      return e;
-    S.G.inv_scale = S.Ht.inv_scale = (float)(1.0 / sc);
-  } else {
-    if (int e = refresh_values(S.G.dev, pos_g_d, g_v_d, ISPM_F64, (long long)nnz_g, 0))
-      return e;
-    if (int e = refresh_values(S.Ht.dev, pos_t_d, gt_v_d, ISPM_F64, (long long)nnz_g, 0))
-      return e;
   }
-  ISPM_CUDA_TRY(cudaMemcpy(&S.fsai_fallbacks, fb_d, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  if (int e = to_device(mem, &f.g_rp, g_rp.data(), g_rp.size()))
+    return e;
+  if (int e = to_device(mem, &f.t_of, t_of.data(), nnz_g))
+    return e;
+  if (int e = to_device(mem, &f.pos_g, pos_g.data(), nnz_g))
+    return e;
+  if (int e = to_device(mem, &f.pos_t, pos_t.data(), nnz_g))
+    return e;
+  if (int e = mem.get(&f.g_v, nnz_g))
+    return e;
+  if (int e = mem.get(&f.gt_v, nnz_g))
+    return e;
+  if (int e = mem.get(&f.fb, 1))
+    return e;
+  if (int e = fsai_values(S, f, a_v_d))
+    return e;
+  if (S.refreshable) {
+    S.fsai = f;
+    S.fsai_kept = true;
+  }
+  return ISPM_OK;
+}
+
+__global__ void gather_values_kernel(double *__restrict__ out, const double *__restrict__ in,
+                                     const int *__restrict__ src, long long n)
+{
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (long long)gridDim.x * blockDim.x)
+    out[k] = in[src[k]];
+}
+
+// ispm_solver_update_values: new values of A in the caller's CSR order.
+int update_values(Solver &S, const double *vals, bool on_device)
+{
+  const long long nnz = S.nnz_a;
+  const double *src = vals;
+  if (!on_device) {
+    double *dst = S.entry_src ? S.a_raw : S.a_v;
+    if (nnz)
+      ISPM_CUDA_TRY(cudaMemcpy(dst, vals, (size_t)nnz * sizeof(double), cudaMemcpyHostToDevice));
+    src = dst;
+  }
+  // the solver's order (renumbered solves)
+  const double *a_v = src;
+  if (S.entry_src) {
+    gather_values_kernel<<<grid_for(nnz), kThreads>>>(S.a_v, src, S.entry_src, nnz);
+    ISPM_CUDA_TRY(cudaPeekAtLastError());
+    a_v = S.a_v;
+  }
+  if (int e = refresh_values(S.A64.dev, S.pos_a64, a_v, ISPM_F64, nnz, 0))
+    return e;
+  if (int e = refresh_values(S.Ain.dev, S.pos_ain, a_v, ISPM_F64, nnz, 0))
+    return e;
+  if (S.fsai_kept)
+    if (int e = fsai_values(S, S.fsai, a_v))
+      return e;
+  ISPM_CUDA_TRY(cudaStreamSynchronize(0));
+  // the iteration graph holds launch arguments by value (an FP16 factor's
+  // scale among them): capture it again at the next solve
+  if (S.graph) {
+    cudaGraphExecDestroy(S.graph);
+    S.graph = nullptr;
+  }
   return ISPM_OK;
 }
 
@@ -1056,6 +1137,7 @@ void ispm_solver_default_opts(ispm_solver_opts *o)
   o->reorder = ISPM_REORDER_AUTO;
   o->matrix_f16 = 0;
   o->factor_f16 = 0;
+  o->refresh = 0;
 }
 
 int ispm_solver_create(int n, const int *row_ptr, const int *cols, const double *vals,
@@ -1112,8 +1194,13 @@ int ispm_solver_create(int n, const int *row_ptr, const int *cols, const double 
   if (S.opts.reorder == ISPM_REORDER_RCM && given_pair)
     return fail(ISPM_ERR_INVALID, "reordering needs prec = ISPM_PREC_FSAI_GPU or none (a given "
                                   "factor pair is in the caller's order)");
+  if (S.opts.refresh && S.inner == ISPM_F32 && S.opts.matrix_f16)
+    return fail(ISPM_ERR_INVALID, "refresh is not available with matrix_f16");
+  S.refreshable = S.opts.refresh != 0;
+  S.nnz_a = row_ptr[n];
   std::vector<int> perm, inv, prp, pci;
   std::vector<double> pv;
+  std::vector<int> entry_src;  // refresh + renumbering: solver entry -> caller entry
   try {
     // automatic mode skips matrices whose band is already under n / 16 (a
     // mesh in its natural order) without computing an ordering
@@ -1129,6 +1216,17 @@ int ispm_solver_create(int n, const int *row_ptr, const int *cols, const double 
       const long long bw1 = bandwidth(n, row_ptr, cols, inv.data());
       // automatic: reorder only a matrix whose numbering is far from banded
       if (S.opts.reorder == ISPM_REORDER_RCM || 4 * bw1 <= bw0) {
+        if (S.refreshable) {
+          // the same permutation applied to the entry indices (exact in FP64)
+          std::vector<double> idx((size_t)S.nnz_a), pidx;
+          std::vector<int> rp2, ci2;
+          for (long long k = 0; k < S.nnz_a; k++)
+            idx[(size_t)k] = (double)k;
+          permute_csr(n, row_ptr, cols, idx.data(), perm, inv, rp2, ci2, pidx);
+          entry_src.resize(pidx.size());
+          for (size_t k = 0; k < pidx.size(); k++)
+            entry_src[k] = (int)pidx[k];
+        }
         permute_csr(n, row_ptr, cols, vals, perm, inv, prp, pci, pv);
         row_ptr = prp.data();
         cols = pci.data();
@@ -1141,10 +1239,14 @@ int ispm_solver_create(int n, const int *row_ptr, const int *cols, const double 
     return fail(ISPM_ERR_NOMEM, "host allocation while reordering");
   }
   try {
+    std::vector<unsigned> pos_ain, pos_a64;
+    std::vector<unsigned> *want_ain = S.refreshable ? &pos_ain : nullptr;
+    std::vector<unsigned> *want_a64 = S.refreshable ? &pos_a64 : nullptr;
     if (S.inner == ISPM_F32 && S.opts.matrix_f16) {
       if (int e = S.Ain.upload_split_f16(n, row_ptr, cols, vals))
         return e;
-    } else if (int e = S.Ain.upload(S.inner, S.inner, n, row_ptr, cols, vals)) {
+    } else if (int e = S.Ain.upload(S.inner, S.inner, n, row_ptr, cols, vals, nullptr,
+                                    want_ain)) {
       return e;
     }
     // the FP64 operator of the reliable updates takes the inner matrix's
@@ -1152,8 +1254,23 @@ int ispm_solver_create(int n, const int *row_ptr, const int *cols, const double 
     // for the off-diagonal part alone): then A64 gets its own min-bytes shape
     const bool split = S.inner == ISPM_F32 && S.opts.matrix_f16;
     if (int e = S.A64.upload(ISPM_F64, ISPM_F64, n, row_ptr, cols, vals,
-                             split ? nullptr : &S.Ain.fmt))
+                             split ? nullptr : &S.Ain.fmt, want_a64))
       return e;
+    if (S.refreshable) {
+      const size_t nnz = (size_t)S.nnz_a;
+      if (int e = to_device(S.mem, &S.pos_ain, pos_ain.data(), nnz))
+        return e;
+      if (int e = to_device(S.mem, &S.pos_a64, pos_a64.data(), nnz))
+        return e;
+      if (int e = S.mem.get(&S.a_v, nnz))
+        return e;
+      if (!entry_src.empty()) {
+        if (int e = to_device(S.mem, &S.entry_src, entry_src.data(), nnz))
+          return e;
+        if (int e = S.mem.get(&S.a_raw, nnz))
+          return e;
+      }
+    }
     if (S.opts.prec == ISPM_PREC_FSAI_GPU) {
       if (int e = build_fsai_on_device(S, n, row_ptr, cols, vals))
         return e;
@@ -1261,6 +1378,16 @@ int ispm_solver_history(const ispm_solver *s, double *out, int cap)
   for (int k = 0; k < n && k < cap; k++)
     out[k] = s->s.history[k];
   return n;
+}
+
+int ispm_solver_update_values(ispm_solver *s, const double *vals, int vals_on_device)
+{
+  clear_error();
+  if (!s || (!vals && s->s.nnz_a))
+    return fail(ISPM_ERR_INVALID, "NULL solver or values");
+  if (!s->s.refreshable)
+    return fail(ISPM_ERR_INVALID, "the solver was created without opts.refresh");
+  return update_values(s->s, vals, vals_on_device != 0);
 }
 
 void ispm_solver_free(ispm_solver *s) { delete s; }

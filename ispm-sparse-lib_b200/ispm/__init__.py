@@ -673,7 +673,7 @@ class solver_opts(C.Structure):
                 ("use_graph", C.c_int), ("replace_ratio_f32", C.c_double),
                 ("replace_ratio_f64", C.c_double), ("variant", C.c_int), ("prec", C.c_int),
                 ("factor_bf16", C.c_int), ("reorder", C.c_int), ("matrix_f16", C.c_int),
-                ("factor_f16", C.c_int)]
+                ("factor_f16", C.c_int), ("refresh", C.c_int)]
 
 
 class solve_stats(C.Structure):
@@ -708,6 +708,8 @@ def _declare_solver():
     L.ispm_solver_history.restype = i
     L.ispm_solver_free.argtypes = [vp]
     L.ispm_solver_free.restype = None
+    L.ispm_solver_update_values.argtypes = [vp, vp, i]
+    L.ispm_solver_update_values.restype = i
     _SOLVER_DECLARED = True
 
 
@@ -719,7 +721,9 @@ class PCGSolver:
     matrices / vectors, FP64 reductions).  Reliable updates recompute the
     true residual with the FP64 matrix whenever the recursive residual has
     fallen by replace_ratio since the previous one.  matrix_f16 (FP32 inner
-    only): the inner iterations use the FP16 split of A (csr_split_f16)."""
+    only): the inner iterations use the FP16 split of A (csr_split_f16).
+    refresh: keep the maps update_values needs (new values of A, same
+    pattern, rewritten on the device)."""
 
     def __init__(self, A: csr_matrix, G1: csr_matrix | None = None,
                  G2: csr_matrix | None = None, inner=np.float32, tol: float = 1e-10,
@@ -727,7 +731,7 @@ class PCGSolver:
                  check_every: int = 16, use_graph: bool = True,
                  replace_ratio: float | None = None, variant: str = "auto",
                  prec: str = "given", factor_bf16: bool = False, reorder: str = "auto",
-                 matrix_f16: bool = False, factor_f16: bool = False):
+                 matrix_f16: bool = False, factor_f16: bool = False, refresh: bool = False):
         _declare_solver()
         L = _lib()
         o = solver_opts()
@@ -743,6 +747,7 @@ class PCGSolver:
         o.reorder = {"none": 0, "rcm": 1, "auto": 2}[reorder]
         o.matrix_f16 = int(matrix_f16)
         o.factor_f16 = int(factor_f16)
+        o.refresh = int(refresh)
         if A.elms.dtype != np.float64:
             raise TypeError("the solver takes the FP64 matrix")
         self._keep = [A, G1, G2]
@@ -795,6 +800,14 @@ class PCGSolver:
         buf = np.zeros(256)
         k = _lib().ispm_solver_history(self._h, _ptr(buf), 256)
         return buf[: min(k, 256)].copy()
+
+    def update_values(self, vals) -> None:
+        """New FP64 values of A in the CSR order given at construction: a numpy
+        array (host) or a CUDA tensor (device).  Needs refresh=True."""
+        on_dev = not isinstance(vals, np.ndarray)
+        if not on_dev:
+            vals = np.ascontiguousarray(vals, np.float64)
+        _check(_lib().ispm_solver_update_values(self._h, _ptr(vals), int(on_dev)))
 
 
 def default_launch_params(m, x_dtype=None) -> spmv_launch_params:
