@@ -46,6 +46,7 @@
 
 #include "cuda_util.cuh"
 #include "fsai.h"
+#include "nvtx_range.h"
 #include "operator.h"
 
 namespace ispm {
@@ -745,6 +746,7 @@ struct Batch {
   int solve_on(const double *b, double *x, ispm_solve_stats *lane_stats, ispm_solve_stats *total,
                cudaStream_t user)
   {
+    NvtxRange range("ispm batch solve");
     ISPM_CUDA_TRY(cudaEventRecord(ev_in, user));
     ISPM_CUDA_TRY(cudaStreamWaitEvent(own, ev_in, 0));
     int e = solve(b, x, lane_stats, total, own);
@@ -1106,6 +1108,7 @@ int ispm_batch_create(int n_systems, const int *n_rows, const int *const *row_pt
                       const ispm_solver_opts *opts, ispm_batch **out)
 {
   clear_error();
+  NvtxRange range("ispm batch create");
   if (!out || n_systems <= 0 || !n_rows || !row_ptr || !cols || !vals || !n_rhs)
     return fail(ISPM_ERR_INVALID, "bad arguments");
   *out = nullptr;

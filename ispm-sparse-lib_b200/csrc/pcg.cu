@@ -40,6 +40,7 @@
 
 #include "cuda_util.cuh"
 #include "fsai.h"
+#include "nvtx_range.h"
 #include "operator.h"
 #include "pcg_state.h"
 #include "sblas_impl.h"
@@ -862,6 +863,7 @@ struct Solver {
       }
       total_it += st_host->it - since_restart;
       since_restart = st_host->it;
+      NvtxRange update_range("ispm reliable update");
       if (int e4 = fold(s))
         return e4;
       if (int e5 = true_residual(s))
@@ -909,6 +911,7 @@ struct Solver {
 
   int solve_on(const double *b, double *x, ispm_solve_stats *stats, cudaStream_t user)
   {
+    NvtxRange range("ispm solve");
     ISPM_CUDA_TRY(cudaEventRecord(ev_in, user));
     ISPM_CUDA_TRY(cudaStreamWaitEvent(own, ev_in, 0));
     int e;
@@ -1080,6 +1083,7 @@ __global__ void gather_values_kernel(double *__restrict__ out, const double *__r
 // ispm_solver_update_values: new values of A in the caller's CSR order.
 int update_values(Solver &S, const double *vals, bool on_device)
 {
+  NvtxRange range("ispm solver update values");
   const long long nnz = S.nnz_a;
   const double *src = vals;
   if (!on_device) {
@@ -1146,6 +1150,7 @@ int ispm_solver_create(int n, const int *row_ptr, const int *cols, const double 
                        const ispm_solver_opts *opts, ispm_solver **out)
 {
   clear_error();
+  NvtxRange range("ispm solver create");
   if (!out || n <= 0 || !row_ptr || !cols || !vals)
     return fail(ISPM_ERR_INVALID, "bad arguments");
   *out = nullptr;

@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "cuda_util.cuh"
+#include "nvtx_range.h"
 #include "spmv_launch.h"
 
 namespace ispm {
@@ -186,6 +187,7 @@ int ispm_plan_create(int vec_dtype, int elm_dtype, int n_rows, int n_cols, const
                      ispm_plan **out)
 {
   clear_error();
+  NvtxRange range("ispm plan create");
   if (!out)
     return fail(ISPM_ERR_INVALID, "out is NULL");
   *out = nullptr;
