@@ -10,6 +10,8 @@
 #ifndef SPMV_GPU_H
 #define SPMV_GPU_H
 
+#include <cuda_runtime.h>
+
 #include "formats/formats.h"
 #include "ispm_compat_detail.h"
 
@@ -52,7 +54,7 @@ template <class E> ispm_c::ispm_slell_view view_of(slell_matrix<E, device_memory
 
 template <class T, class E>
 void launch(const spmv_launch_params &params, slell_matrix<E, device_memory_space_tag> &m,
-            T *x, T *y)
+            T *x, T *y, cudaStream_t stream = NULL)
 {
   static_assert(sizeof(T) >= sizeof(E) && (sizeof(E) == 4 || sizeof(E) == 8),
                 "launch_spmv_kernel<T, E>: (float, float), (double, float) or (double, double)");
@@ -63,7 +65,7 @@ void launch(const spmv_launch_params &params, slell_matrix<E, device_memory_spac
   p.use_tex_sliceptr = params.use_tex_sliceptr;
   p.use_tex_x = params.use_tex_x;
   const ispm_c::ispm_slell_view v = view_of(m);
-  const int st = ispm_c::ispm_launch_spmv(dtype_of<T>::value, &p, &v, x, y, NULL);
+  const int st = ispm_c::ispm_launch_spmv(dtype_of<T>::value, &p, &v, x, y, stream);
   if (st != ISPM_ERR_INVALID)  // unsupported parameters: nothing launched
     check(st, "launch_spmv_kernel");
 }
@@ -83,6 +85,23 @@ void launch_spmv_kernel(spmv_launch_params &params, slell_matrix<E, device_memor
                         T *xptr, T *yptr)
 {
   ispm_compat::launch<T, E>(params, m, xptr, yptr);
+}
+
+/* Additions to the reference's interface: the same launches ordered on a
+ * caller's stream (asynchronous with the host). */
+template <class T, class E>
+void launch_spmv_kernel(spmv_launch_params &params, slell_matrix<E, device_memory_space_tag> &m,
+                        vector<T, device_memory_space_tag> &x,
+                        vector<T, device_memory_space_tag> &y, cudaStream_t stream)
+{
+  ispm_compat::launch<T, E>(params, m, x.udata(), y.udata(), stream);
+}
+
+template <class T, class E>
+void launch_spmv_kernel(spmv_launch_params &params, slell_matrix<E, device_memory_space_tag> &m,
+                        T *xptr, T *yptr, cudaStream_t stream)
+{
+  ispm_compat::launch<T, E>(params, m, xptr, yptr, stream);
 }
 
 #endif

@@ -190,6 +190,19 @@ int main()
   launch_spmv_kernel<double, double>(p4, dB, x.udata(), y2.udata());
   yh = y2;
   expect(close(yh, 1e-14), "spmv<double,double> pointer overload");
+  {
+    // the drop-in headers' stream overloads (no counterpart in the reference)
+    cudaStream_t st;
+    cudaStreamCreate(&st);
+    vector<double, device_memory_space_tag> y5(n);
+    launch_spmv_kernel<double, double>(p4, dB, x, y5, st);
+    vector<double, device_memory_space_tag> s5(1);
+    sblas::dot<double>(x.data(), y5.data(), s5.data(), n, st);
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    vector<double, host_memory_space_tag> y5h(y5);
+    expect(close(y5h, 1e-14), "spmv<double,double> on a stream");
+  }
   // unsupported parameters launch nothing (y2 keeps its values)
   spmv_launch_params bad = {4, 32, 1, true, true};
   vector<double, device_memory_space_tag> y3(yh);
