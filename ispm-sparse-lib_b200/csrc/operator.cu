@@ -1,8 +1,12 @@
 // Solver operators (operator.h).
 #include "operator.h"
 
+#include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
+#include <new>
+#include <thread>
 #include <utility>
 
 #include "cuda_util.cuh"
@@ -42,6 +46,70 @@ const void *typed_values(int elm_dtype, const double *v, size_t nnz, std::vector
   return vf.data();
 }
 
+// Convert the CSR into every candidate shape and keep the one with the
+// fewest stored bytes (the earliest candidate on a tie).  The conversions
+// are independent host passes over the matrix, so they run on up to one
+// thread per core; each thread keeps only its own best, so at most that
+// many converted copies exist at once.  Returns the index of the chosen
+// candidate, or -1 when no shape accepted the matrix (with one candidate,
+// the conversion's own error message stands).
+int convert_smallest(int elm_dtype, int n_rows, int n_cols, const int *rp, const int *ci,
+                     const void *vals, const std::vector<ispm_slell_params> &cands,
+                     HostSlell &best, size_t &best_bytes)
+{
+  struct Best {
+    int idx = -1;
+    size_t bytes = ~(size_t)0;
+    HostSlell h;
+  };
+  auto consider = [](Best &b, int idx, size_t bytes) {
+    return b.idx < 0 || bytes < b.bytes || (bytes == b.bytes && idx < b.idx);
+  };
+  const int nc = (int)cands.size();
+  unsigned hw = std::thread::hardware_concurrency();
+  const int nt = std::max(1, std::min(nc, (int)(hw ? hw : 1)));
+  std::vector<Best> local(nt);
+  std::atomic<int> next{0};
+  auto work = [&](int t) {
+    for (int k = next.fetch_add(1); k < nc; k = next.fetch_add(1)) {
+      const ispm_slell_params &c = cands[k];
+      HostSlell h;
+      try {
+        if (convert_csr(elm_dtype, n_rows, n_cols, rp, ci, vals, (int)c.S, (int)c.H, c.V != 0,
+                        c.D != 0, 4, h))
+          continue;
+      } catch (const std::bad_alloc &) {
+        continue;
+      }
+      const size_t bytes = stored_bytes(h);
+      if (consider(local[t], k, bytes)) {
+        local[t].idx = k;
+        local[t].bytes = bytes;
+        local[t].h = std::move(h);
+      }
+    }
+  };
+  if (nt == 1) {
+    work(0);
+  } else {
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; t++)
+      pool.emplace_back(work, t);
+    work(0);
+    for (std::thread &th : pool)
+      th.join();
+  }
+  int bi = -1;
+  for (int t = 0; t < nt; t++)
+    if (local[t].idx >= 0 && (bi < 0 || consider(local[bi], local[t].idx, local[t].bytes)))
+      bi = t;
+  if (bi < 0)
+    return -1;
+  best = std::move(local[bi].h);
+  best_bytes = local[bi].bytes;
+  return local[bi].idx;
+}
+
 }  // namespace
 
 int choose_format(int elm_dtype, int n_rows, int n_cols, const int *rp, const int *ci,
@@ -51,21 +119,13 @@ int choose_format(int elm_dtype, int n_rows, int n_cols, const int *rp, const in
   const void *vals = typed_values(elm_dtype, v, (size_t)rp[n_rows], vf);
   std::vector<ispm_slell_params> cands;
   candidate_shapes(elm_dtype, n_rows, n_cols, rp, ci, vals, fixed_height, cands);
-  size_t best = ~(size_t)0;
-  for (const ispm_slell_params &c : cands) {
-    HostSlell h;
-    if (convert_csr(elm_dtype, n_rows, n_cols, rp, ci, vals, (int)c.S, (int)c.H, c.V != 0,
-                    c.D != 0, 4, h))
-      continue;
-    const size_t bytes = stored_bytes(h);
-    if (bytes < best) {
-      best = bytes;
-      out = c;
-    }
-  }
+  HostSlell h;
+  size_t best = 0;
+  const int k = convert_smallest(elm_dtype, n_rows, n_cols, rp, ci, vals, cands, h, best);
   clear_error();
-  if (best == ~(size_t)0)
+  if (k < 0)
     return fail(ISPM_ERR_INVALID, "no sliced-ELL shape accepted the matrix");
+  out = cands[k];
   if (out_bytes)
     *out_bytes = best;
   return ISPM_OK;
@@ -85,22 +145,12 @@ int Operator::upload(int vec_dtype, int elm_dtype, int n, const int *rp, const i
     candidate_shapes(elm_dtype, n, n, rp, ci, vals, fixed_height, cands);
   // convert every candidate and keep the smallest (no second conversion)
   HostSlell best;
-  size_t best_bytes = ~(size_t)0;
-  for (const ispm_slell_params &c : cands) {
-    HostSlell h;
-    if (convert_csr(elm_dtype, n, n, rp, ci, vals, (int)c.S, (int)c.H, c.V != 0, c.D != 0, 4,
-                    h))
-      continue;
-    const size_t bytes = stored_bytes(h);
-    if (bytes < best_bytes) {
-      best_bytes = bytes;
-      best = std::move(h);
-      fmt = c;
-    }
-  }
-  if (best_bytes == ~(size_t)0)
+  size_t best_bytes = 0;
+  const int k = convert_smallest(elm_dtype, n, n, rp, ci, vals, cands, best, best_bytes);
+  if (k < 0)
     return force ? ISPM_ERR_INVALID  // the conversion's own message stands
                  : fail(ISPM_ERR_INVALID, "no sliced-ELL shape accepted the operator");
+  fmt = cands[k];
   clear_error();
   if (value_pos)
     if (int st = value_map(best, n, rp, ci, *value_pos))
