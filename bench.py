@@ -660,28 +660,36 @@ def c3_compact(ispm, gen, torch, stream, tol, steps=3):
     t0 = time.time()
     A = gen.unstructured(192, 0.05, 1, 0.1, 10.0, 1.01)
     b = oracle_spmv(A, np.random.default_rng(0).uniform(-1, 1, A.n_rows))
-    A32 = ispm.csr_matrix(A.n_rows, A.n_cols, A.row_ptr, A.cols, A.elms.astype(np.float32))
-    plan = ispm.spmv_plan(A32, ispm.PLAN_EXHAUSTIVE, T=np.float32)
-    mp, lp = plan.mparams, plan.params
-    view = plan.host_matrix.view()
-    xs = torch.rand(A.n_cols, dtype=torch.float32, device="cuda")
-    ys = torch.zeros(view.n_rows, dtype=torch.float32, device="cuda")
-    for _ in range(5):
-        plan.execute_spmv(xs, ys, stream)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(30):
-        plan.execute_spmv(xs, ys, stream)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    t_spmv = e0.elapsed_time(e1) / 30 * 1e-3
-    alg = algorithmic_bytes(view, 4)
     peak, _ = measured_peak()
-    del plan
+
+    def plan_spmv(M):
+        """FP32 SpMV of M in the exhaustive plan's shape, live."""
+        M32 = ispm.csr_matrix(M.n_rows, M.n_cols, M.row_ptr, M.cols, M.elms.astype(np.float32))
+        plan = ispm.spmv_plan(M32, ispm.PLAN_EXHAUSTIVE, T=np.float32)
+        mp, lp = plan.mparams, plan.params
+        view = plan.host_matrix.view()
+        xs = torch.rand(M.n_cols, dtype=torch.float32, device="cuda")
+        ys = torch.zeros(view.n_rows, dtype=torch.float32, device="cuda")
+        for _ in range(5):
+            plan.execute_spmv(xs, ys, stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(30):
+            plan.execute_spmv(xs, ys, stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t_spmv = e0.elapsed_time(e1) / 30 * 1e-3
+        alg = algorithmic_bytes(view, 4)
+        del plan
+        return {"S": mp.S, "hblock": mp.H, "var_height": mp.V, "diags": mp.D, "N": lp.N,
+                "H": lp.H, "us": t_spmv * 1e6, "algorithmic_bytes": alg,
+                "achieved_gbs": alg / t_spmv / 1e9, "frac": alg / t_spmv / 1e9 / peak,
+                "bandwidth": ispm.csr_bandwidth(M)}
+
     out = {"workload": C3_WORKLOAD, "rows": A.n_rows, "nnz": A.n_nz, "tol": tol,
-           "spmv": {"S": mp.S, "hblock": mp.H, "var_height": mp.V, "diags": mp.D, "N": lp.N,
-                    "H": lp.H, "us": t_spmv * 1e6, "algorithmic_bytes": alg,
-                    "achieved_gbs": alg / t_spmv / 1e9, "frac": alg / t_spmv / 1e9 / peak}}
+           "spmv": plan_spmv(A),
+           # the numbering the solver iterates in (reverse Cuthill-McKee)
+           "spmv_renumbered": plan_spmv(ispm.permute_symmetric(A, ispm.rcm_order(A)))}
     for name, kw in (("mixed", dict(inner=np.float32)),
                      ("plain_fp64", dict(inner=np.float64, variant="pipelined"))):
         S = ispm.PCGSolver(A, tol=tol, prec="fsai_gpu", **kw)

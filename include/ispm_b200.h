@@ -340,6 +340,13 @@ int ispm_fsai_sym_gpu(int out_dtype, int n, const int *row_ptr, const int *cols,
  * rounding errors (zero row sums for an M-matrix).  scale is the power of
  * two that maps the largest off-diagonal magnitude into [2^13, 2^14).
  * off_f16 has row_ptr[n] entries, diag n. */
+/* Reverse Cuthill-McKee ordering of a symmetric n x n pattern (no
+ * counterpart in the reference; the solver's opts.reorder uses it):
+ * perm[new] = old, n entries.  The renumbered matrix P A P^T keeps each
+ * row's neighbours in a narrow band, so SpMV gathers of x become local. */
+int ispm_rcm_order(int n, const int *row_ptr, const int *cols, int *perm);
+/* max |col - row| over the pattern, or -1 for a malformed CSR. */
+long long ispm_csr_bandwidth(int n, const int *row_ptr, const int *cols);
 int ispm_csr_split_f16(int n, const int *row_ptr, const int *cols, const double *vals,
                        uint16_t *off_f16, float *diag, float *scale);
 int ispm_csr_get_info(const ispm_csr *m, int *n_rows, int *n_cols, int *n_nz, int *dtype);

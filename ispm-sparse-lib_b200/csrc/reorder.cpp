@@ -3,6 +3,7 @@
 // randomly permuted mesh): with the rows renumbered, the x gathers of every
 // SpMV land in a narrow band again instead of anywhere in the vector.
 #include <algorithm>
+#include <new>
 #include <vector>
 
 #include "ispm_internal.h"
@@ -121,3 +122,28 @@ void permute_csr(int n, const int *rp, const int *ci, const double *v,
 }
 
 }  // namespace ispm
+
+extern "C" int ispm_rcm_order(int n, const int *row_ptr, const int *cols, int *perm)
+{
+  ispm::clear_error();
+  if (n < 0 || !row_ptr || !perm)
+    return ispm::fail(ISPM_ERR_INVALID, "bad arguments");
+  if (int e = ispm::validate_csr(n, n, row_ptr, cols))
+    return e;
+  try {
+    std::vector<int> p;
+    ispm::rcm_order(n, row_ptr, cols, p);
+    std::copy(p.begin(), p.end(), perm);
+  } catch (const std::bad_alloc &) {
+    return ispm::fail(ISPM_ERR_NOMEM, "host allocation");
+  }
+  return ISPM_OK;
+}
+
+extern "C" long long ispm_csr_bandwidth(int n, const int *row_ptr, const int *cols)
+{
+  ispm::clear_error();
+  if (n < 0 || !row_ptr || ispm::validate_csr(n, n, row_ptr, cols))
+    return -1;
+  return ispm::bandwidth(n, row_ptr, cols, nullptr);
+}

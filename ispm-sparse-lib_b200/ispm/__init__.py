@@ -401,6 +401,38 @@ def launch_spmv_kernel(params: spmv_launch_params, m, x, y, stream=None):
                                    _ptr(y), _stream(stream)))
 
 
+def rcm_order(A: csr_matrix) -> np.ndarray:
+    """Reverse Cuthill-McKee ordering of A's (symmetric) pattern: perm[new] = old."""
+    L = _lib()
+    L.ispm_rcm_order.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.ispm_rcm_order.restype = C.c_int
+    perm = np.zeros(max(A.n_rows, 1), np.int32)
+    _check(L.ispm_rcm_order(A.n_rows, _ptr(A.row_ptr), _ptr(A.cols), _ptr(perm)))
+    return perm[: A.n_rows]
+
+
+def csr_bandwidth(A: csr_matrix) -> int:
+    """max |col - row| over A's pattern."""
+    L = _lib()
+    L.ispm_csr_bandwidth.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
+    L.ispm_csr_bandwidth.restype = C.c_longlong
+    bw = L.ispm_csr_bandwidth(A.n_rows, _ptr(A.row_ptr), _ptr(A.cols))
+    if bw < 0:
+        _check(ERR_INVALID)
+    return int(bw)
+
+
+def permute_symmetric(A: csr_matrix, perm: np.ndarray) -> csr_matrix:
+    """P A P^T with perm[new] = old (rows and columns renumbered, columns
+    sorted within each row)."""
+    import scipy.sparse as sp
+    M = sp.csr_matrix((A.elms, A.cols, A.row_ptr), shape=(A.n_rows, A.n_cols))
+    M = M[perm][:, perm].tocsr()
+    M.sort_indices()
+    return csr_matrix(A.n_rows, A.n_cols, M.indptr.astype(np.int32),
+                      M.indices.astype(np.int32), M.data.astype(A.elms.dtype))
+
+
 def csr_split_f16(A: csr_matrix):
     """The FP16 split the solver's matrix_f16 option stores: (off, diag,
     scale) with off[k] the binary16 bit pattern (uint16) of A's CSR entry k

@@ -6,6 +6,7 @@ import os
 import re
 
 import numpy as np
+import pytest
 
 from conftest import PKG, ROOT
 
@@ -113,3 +114,29 @@ def test_solver_rejects_malformed_csr_before_reordering(ispm, gen):
         ispm.PCGSolver(A, ispm.csr_matrix(A.n_rows, A.n_cols, A.row_ptr, bad_col, A.elms), A,
                        inner=np.float64)
     assert e.value.status == ispm.ERR_INVALID
+
+
+def test_rcm_order_is_a_permutation_that_narrows_the_band(ispm, gen):
+    """ispm_rcm_order on a randomly numbered mesh: perm is a permutation and
+    the renumbered matrix's bandwidth is far below the scattered one's;
+    malformed patterns are refused."""
+    A = gen.unstructured(12, 0.05, 3, 0.1, 10.0, 1.01)
+    perm = ispm.rcm_order(A)
+    assert np.array_equal(np.sort(perm), np.arange(A.n_rows))
+    B = ispm.permute_symmetric(A, perm)
+    assert B.row_ptr[-1] == A.row_ptr[-1]
+    assert ispm.csr_bandwidth(B) * 4 <= ispm.csr_bandwidth(A)
+    # P A P^T holds the same entries: (B x)[i] = (A x_perm)[perm[i]]
+    x = np.random.default_rng(1).uniform(-1, 1, A.n_rows)
+    import scipy.sparse as sp
+    MA = sp.csr_matrix((A.elms, A.cols, A.row_ptr), shape=(A.n_rows, A.n_rows))
+    MB = sp.csr_matrix((B.elms, B.cols, B.row_ptr), shape=(A.n_rows, A.n_rows))
+    xa = np.empty_like(x)
+    xa[perm] = x
+    assert np.allclose(MB @ x, (MA @ xa)[perm], rtol=1e-14, atol=1e-14)
+    bad = ispm.csr_matrix(3, 3, np.array([0, 1, 2, 3], np.int32), np.array([0, 5, 2], np.int32),
+                          np.ones(3))
+    with pytest.raises(ispm.IspmError):
+        ispm.rcm_order(bad)
+    with pytest.raises(ispm.IspmError):
+        ispm.csr_bandwidth(bad)
