@@ -47,23 +47,26 @@ const void *typed_values(int elm_dtype, const double *v, size_t nnz, std::vector
 }
 
 // Convert the CSR into every candidate shape and keep the one with the
-// fewest stored bytes (the earliest candidate on a tie).  The conversions
-// are independent host passes over the matrix, so they run on up to one
-// thread per core; each thread keeps only its own best, so at most that
-// many converted copies exist at once.  Returns the index of the chosen
+// fewest stored bytes, each candidate's bytes times weight[k] when weights
+// are given (the earliest candidate on a tie).  The conversions are
+// independent host passes over the matrix, so they run on up to one thread
+// per core; each thread keeps only its own best, so at most that many
+// converted copies exist at once.  Returns the index of the chosen
 // candidate, or -1 when no shape accepted the matrix (with one candidate,
 // the conversion's own error message stands).
 int convert_smallest(int elm_dtype, int n_rows, int n_cols, const int *rp, const int *ci,
                      const void *vals, const std::vector<ispm_slell_params> &cands,
-                     HostSlell &best, size_t &best_bytes)
+                     HostSlell &best, size_t &best_bytes,
+                     const std::vector<double> *weight = nullptr)
 {
   struct Best {
     int idx = -1;
+    double cost = 0.0;
     size_t bytes = ~(size_t)0;
     HostSlell h;
   };
-  auto consider = [](Best &b, int idx, size_t bytes) {
-    return b.idx < 0 || bytes < b.bytes || (bytes == b.bytes && idx < b.idx);
+  auto consider = [](const Best &b, int idx, double cost) {
+    return b.idx < 0 || cost < b.cost || (cost == b.cost && idx < b.idx);
   };
   const int nc = (int)cands.size();
   unsigned hw = std::thread::hardware_concurrency();
@@ -82,8 +85,10 @@ int convert_smallest(int elm_dtype, int n_rows, int n_cols, const int *rp, const
         continue;
       }
       const size_t bytes = stored_bytes(h);
-      if (consider(local[t], k, bytes)) {
+      const double cost = (double)bytes * (weight ? (*weight)[k] : 1.0);
+      if (consider(local[t], k, cost)) {
         local[t].idx = k;
+        local[t].cost = cost;
         local[t].bytes = bytes;
         local[t].h = std::move(h);
       }
@@ -101,7 +106,7 @@ int convert_smallest(int elm_dtype, int n_rows, int n_cols, const int *rp, const
   }
   int bi = -1;
   for (int t = 0; t < nt; t++)
-    if (local[t].idx >= 0 && (bi < 0 || consider(local[bi], local[t].idx, local[t].bytes)))
+    if (local[t].idx >= 0 && (bi < 0 || consider(local[bi], local[t].idx, local[t].cost)))
       bi = t;
   if (bi < 0)
     return -1;
@@ -143,10 +148,22 @@ int Operator::upload(int vec_dtype, int elm_dtype, int n, const int *rp, const i
     cands.push_back(*force);
   else
     candidate_shapes(elm_dtype, n, n, rp, ci, vals, fixed_height, cands);
-  // convert every candidate and keep the smallest (no second conversion)
+  // convert every candidate and keep the smallest (no second conversion).
+  // Short slices cost time that their stored bytes do not show: at the
+  // default 4 rows a thread a 32-row slice is 8 threads, so a warp walks
+  // four slices' diagonal lists and x windows, where a 128-row slice is one
+  // warp.  Measured on a B200 (FP32, diagonal blocks): the renumbered 192^3
+  // 7-point graph's A takes 82.5 us at S = 32 (its fewest bytes) and 74.8 us
+  // at S = 128 (4% more bytes), its FSAI factor 49.3 / 45.8 us (3% more);
+  // the 128^3 27-point A 45.5 us at S = 64 and 43.6 us at S = 128.  So
+  // 32-row shapes count 10% and 64-row shapes 2% above their bytes.
+  std::vector<double> weight(cands.size(), 1.0);
+  for (size_t c = 0; c < cands.size(); c++)
+    weight[c] = cands[c].S <= 32 ? 1.10 : cands[c].S == 64 ? 1.02 : 1.0;
   HostSlell best;
   size_t best_bytes = 0;
-  const int k = convert_smallest(elm_dtype, n, n, rp, ci, vals, cands, best, best_bytes);
+  const int k =
+      convert_smallest(elm_dtype, n, n, rp, ci, vals, cands, best, best_bytes, &weight);
   if (k < 0)
     return force ? ISPM_ERR_INVALID  // the conversion's own message stands
                  : fail(ISPM_ERR_INVALID, "no sliced-ELL shape accepted the operator");
