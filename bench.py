@@ -92,8 +92,9 @@ def launch_override(ispm, args, p):
 
 
 def kernel_only(args):
-    """Upload the workload matrix in the guessed format and launch its SpMV
-    --reps times with the DEFAULT plan's launch shape."""
+    """Upload the workload matrix in the shape the solver stores it in
+    (ispm_solver_choose_shape) and launch its SpMV --reps times with the
+    default launch shape (or --launch)."""
     import torch
     import ispm
     import ispm.gen as gen
@@ -111,7 +112,7 @@ def kernel_only(args):
         return
     dt = np.float32 if args.kernel_only == "spmv32" else np.float64
     Ae = ispm.csr_matrix(A.n_rows, A.n_cols, A.row_ptr, A.cols, A.elms.astype(dt))
-    B = ispm.csr_to_slell_guess_format(Ae)
+    B = ispm.csr_to_slell(Ae, *ispm.solver_shape(A, dt))  # the solver's own shape
     d = B.upload()
     del B
     p = launch_override(ispm, args, ispm.default_launch_params(d, dt))
@@ -899,14 +900,13 @@ def main():
     e2e = (time.perf_counter() - t0) / args.steps
     relres_e2e = float(np.linalg.norm(b - oracle_spmv(A, pin_x.numpy())) / np.linalg.norm(b))
 
-    # dominant kernel: the SpMV of A inside the mixed solve, FP32-stored and
-    # FP16-split, each timed alone (the headline's storage is the roofline line)
-    A32 = ispm.csr_matrix(A.n_rows, A.n_cols, A.row_ptr, A.cols, A.elms.astype(np.float32))
-    B32 = ispm.csr_to_slell_guess_format(A32)
-    d32 = B32.upload()
+    # dominant kernel: the SpMV of A inside the mixed solve, FP32-stored (the
+    # solver's own device matrix and launch shape) and FP16-split, each timed
+    # alone (the headline's storage is the roofline line)
+    v32, p32 = (alt if f16 else best).operator(0)
     d16 = ispm.device_split_f16(A)
     xs = torch.rand(A.n_cols, dtype=torch.float32, device="cuda")
-    ys = torch.zeros(B32.n_rows, dtype=torch.float32, device="cuda")
+    ys = torch.zeros(v32.n_rows, dtype=torch.float32, device="cuda")
     reps = 50
 
     def time_spmv(launch):
@@ -920,12 +920,11 @@ def main():
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / reps * 1e-3
 
-    p32 = ispm.default_launch_params(d32, np.float32)
     p16 = ispm.default_launch_params(d16, np.float32)
-    t32 = time_spmv(lambda: ispm.launch_spmv_kernel(p32, d32, xs, ys, stream))
+    t32 = time_spmv(lambda: ispm.launch_spmv_kernel(p32, v32, xs, ys, stream))
     ys16 = torch.zeros(d16.view().n_rows, dtype=torch.float32, device="cuda")
     t16 = time_spmv(lambda: d16.apply(p16, xs, ys16, stream))
-    alg32 = algorithmic_bytes(B32.view(), 4)
+    alg32 = algorithmic_bytes(v32, 4)
     alg16 = algorithmic_bytes(d16.view(), 4, split_rows=d16.view().n_rows)
     peak, peak_src = measured_peak()
     if f16:

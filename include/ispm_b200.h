@@ -473,6 +473,21 @@ int ispm_solver_solve_host(ispm_solver *s, const double *b_host, double *x_host,
  * breakdown in the next solve).  Synchronous.  (The reference's
  * counterpart for one matrix is spmv_plan::refresh_values, plan/plan.h:39-56.) */
 int ispm_solver_update_values(ispm_solver *s, const double *vals, int vals_on_device);
+/* The device matrices the solver iterates with, for inspection or a
+ * caller's own products: which = 0 the inner-precision A, 1 the FP64 A of
+ * the reliable updates, 2 G, 3 G^T (in the solver's numbering when it
+ * renumbered); *view gets the device view, *params (may be NULL) the launch
+ * shape the solver uses.  Valid until ispm_solver_free. */
+int ispm_solver_operator(const ispm_solver *s, int which, ispm_slell_view *view,
+                         ispm_launch_params *params);
+/* The sliced-ELL shape the solver stores an n x n operator in (elm_dtype
+ * ISPM_F32 or ISPM_F64): among the reference's guessed format and the fixed
+ * heights 32 / 64 / 128 with and without diagonal blocks (and hblock 2),
+ * the fewest stored bytes, with 32- and 64-row slices counted 10% / 2%
+ * above their bytes (measured on a B200: short slices cost time their
+ * bytes do not show).  Host only. */
+int ispm_solver_choose_shape(int elm_dtype, int n, const int *row_ptr, const int *cols,
+                             const double *vals, ispm_slell_params *out);
 /* True relative residual after each outer cycle of the last solve; returns
  * the count (writes at most cap values). */
 int ispm_solver_history(const ispm_solver *s, double *out, int cap);

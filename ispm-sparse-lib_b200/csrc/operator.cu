@@ -115,7 +115,34 @@ int convert_smallest(int elm_dtype, int n_rows, int n_cols, const int *rp, const
   return local[bi].idx;
 }
 
+// The solver operators' cost weights per candidate shape (Operator::upload).
+std::vector<double> shape_weights(const std::vector<ispm_slell_params> &cands)
+{
+  std::vector<double> w(cands.size(), 1.0);
+  for (size_t c = 0; c < cands.size(); c++)
+    w[c] = cands[c].S <= 32 ? 1.10 : cands[c].S == 64 ? 1.02 : 1.0;
+  return w;
+}
+
 }  // namespace
+
+int choose_operator_shape(int elm_dtype, int n, const int *rp, const int *ci, const double *v,
+                          ispm_slell_params &out)
+{
+  std::vector<float> vf;
+  const void *vals = typed_values(elm_dtype, v, (size_t)rp[n], vf);
+  std::vector<ispm_slell_params> cands;
+  candidate_shapes(elm_dtype, n, n, rp, ci, vals, false, cands);
+  const std::vector<double> weight = shape_weights(cands);
+  HostSlell h;
+  size_t bytes = 0;
+  const int k = convert_smallest(elm_dtype, n, n, rp, ci, vals, cands, h, bytes, &weight);
+  clear_error();
+  if (k < 0)
+    return fail(ISPM_ERR_INVALID, "no sliced-ELL shape accepted the matrix");
+  out = cands[k];
+  return ISPM_OK;
+}
 
 int choose_format(int elm_dtype, int n_rows, int n_cols, const int *rp, const int *ci,
                   const double *v, bool fixed_height, ispm_slell_params &out, size_t *out_bytes)
@@ -157,9 +184,7 @@ int Operator::upload(int vec_dtype, int elm_dtype, int n, const int *rp, const i
   // at S = 128 (4% more bytes), its FSAI factor 49.3 / 45.8 us (3% more);
   // the 128^3 27-point A 45.5 us at S = 64 and 43.6 us at S = 128.  So
   // 32-row shapes count 10% and 64-row shapes 2% above their bytes.
-  std::vector<double> weight(cands.size(), 1.0);
-  for (size_t c = 0; c < cands.size(); c++)
-    weight[c] = cands[c].S <= 32 ? 1.10 : cands[c].S == 64 ? 1.02 : 1.0;
+  const std::vector<double> weight = shape_weights(cands);
   HostSlell best;
   size_t best_bytes = 0;
   const int k =

@@ -22,6 +22,10 @@ namespace ispm {
 int choose_format(int elm_dtype, int n_rows, int n_cols, const int *rp, const int *ci,
                   const double *v, bool fixed_height, ispm_slell_params &out,
                   size_t *out_bytes = nullptr);
+// The shape Operator::upload picks for an n x n operator without a forced
+// shape (fewest stored bytes, short slices weighted up).
+int choose_operator_shape(int elm_dtype, int n, const int *rp, const int *ci, const double *v,
+                          ispm_slell_params &out);
 
 // IEEE binary16 of v, rounded to nearest even (subnormals kept); |v| must be
 // below 65520 (the binary16 overflow threshold).

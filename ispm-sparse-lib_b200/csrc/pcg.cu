@@ -1385,6 +1385,40 @@ int ispm_solver_history(const ispm_solver *s, double *out, int cap)
   return n;
 }
 
+int ispm_solver_choose_shape(int elm_dtype, int n, const int *row_ptr, const int *cols,
+                             const double *vals, ispm_slell_params *out)
+{
+  clear_error();
+  if (!out || n <= 0 || !row_ptr || !vals || (elm_dtype != ISPM_F32 && elm_dtype != ISPM_F64))
+    return fail(ISPM_ERR_INVALID, "bad arguments");
+  if (int e = validate_csr(n, n, row_ptr, cols))
+    return e;
+  try {
+    return choose_operator_shape(elm_dtype, n, row_ptr, cols, vals, *out);
+  } catch (const std::bad_alloc &) {
+    return fail(ISPM_ERR_NOMEM, "host allocation");
+  }
+}
+
+int ispm_solver_operator(const ispm_solver *s, int which, ispm_slell_view *view,
+                         ispm_launch_params *params)
+{
+  clear_error();
+  if (!s || !view)
+    return fail(ISPM_ERR_INVALID, "NULL argument");
+  const Solver &S = s->s;
+  const Operator *op = which == 0 ? &S.Ain : which == 1 ? &S.A64 : which == 2 ? &S.G
+                     : which == 3 ? &S.Ht : nullptr;
+  if (!op)
+    return fail(ISPM_ERR_INVALID, "operator %d (0 inner A, 1 FP64 A, 2 G, 3 G^T)", which);
+  if (which >= 2 && !S.have_prec)
+    return fail(ISPM_ERR_INVALID, "the solver has no preconditioner");
+  *view = op->dev.view();
+  if (params)
+    *params = op->lp;
+  return ISPM_OK;
+}
+
 int ispm_solver_update_values(ispm_solver *s, const double *vals, int vals_on_device)
 {
   clear_error();

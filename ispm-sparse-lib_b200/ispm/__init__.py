@@ -401,6 +401,21 @@ def launch_spmv_kernel(params: spmv_launch_params, m, x, y, stream=None):
                                    _ptr(y), _stream(stream)))
 
 
+def solver_shape(A: csr_matrix, elm_dtype=np.float32) -> tuple:
+    """(S, hblock, var_height, diags): the shape the solver stores the n x n
+    operator A in with elm_dtype elements (ispm_solver_choose_shape)."""
+    L = _lib()
+    L.ispm_solver_choose_shape.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.POINTER(slell_params)]
+    L.ispm_solver_choose_shape.restype = C.c_int
+    v = np.ascontiguousarray(A.elms, np.float64)
+    p = slell_params()
+    _check(L.ispm_solver_choose_shape(F32 if np.dtype(elm_dtype) == np.float32 else F64,
+                                      A.n_rows, _ptr(A.row_ptr), _ptr(A.cols), _ptr(v),
+                                      C.byref(p)))
+    return (p.S, p.H, p.V, p.D)
+
+
 def rcm_order(A: csr_matrix) -> np.ndarray:
     """Reverse Cuthill-McKee ordering of A's (symmetric) pattern: perm[new] = old."""
     L = _lib()
@@ -832,6 +847,17 @@ class PCGSolver:
         buf = np.zeros(256)
         k = _lib().ispm_solver_history(self._h, _ptr(buf), 256)
         return buf[: min(k, 256)].copy()
+
+    def operator(self, which: int = 0):
+        """(view, launch params) of the device matrix the solver iterates
+        with: 0 inner A, 1 FP64 A, 2 G, 3 G^T."""
+        L = _lib()
+        L.ispm_solver_operator.argtypes = [C.c_void_p, C.c_int, C.POINTER(slell_view),
+                                           C.POINTER(spmv_launch_params)]
+        L.ispm_solver_operator.restype = C.c_int
+        v, p = slell_view(), spmv_launch_params()
+        _check(L.ispm_solver_operator(self._h, which, C.byref(v), C.byref(p)))
+        return v, p
 
     def update_values(self, vals) -> None:
         """New FP64 values of A in the CSR order given at construction: a numpy

@@ -140,3 +140,18 @@ def test_rcm_order_is_a_permutation_that_narrows_the_band(ispm, gen):
         ispm.rcm_order(bad)
     with pytest.raises(ispm.IspmError):
         ispm.csr_bandwidth(bad)
+
+
+def test_solver_shape(ispm, gen):
+    """ispm_solver_choose_shape: a shape the conversion accepts, and on a
+    27-point grid the 128-row diagonal-block shape (fewest bytes there)."""
+    A = gen.stencil_grf(24, 27, 4.0, 1.5, 1)
+    s = ispm.solver_shape(A)
+    assert s == (128, 1, 0, 1)
+    U = gen.unstructured(10, 0.05, 3, 0.1, 10.0, 1.01)
+    S, H, V, D = ispm.solver_shape(U, np.float64)
+    ispm.csr_to_slell(U, S, H, V, D)  # accepted
+    bad = ispm.csr_matrix(3, 3, np.array([0, 1, 2, 3], np.int32), np.array([0, 5, 2], np.int32),
+                          np.ones(3))
+    with pytest.raises(ispm.IspmError):
+        ispm.solver_shape(bad)
