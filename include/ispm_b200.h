@@ -406,7 +406,9 @@ typedef struct {
                            scale (the largest magnitude lands in [2^13, 2^14)),
                            11 mantissa bits where BF16 keeps 8; half the bytes
                            of each factor application.  Takes precedence over
-                           factor_bf16. */
+                           factor_bf16.  On by default (the 128^3 27-point
+                           solve: 59.4 against 61.9 ms with FP32 factors,
+                           499 against 501 iterations, on a B200). */
   int refresh;          /* keep what ispm_solver_update_values needs to take new
                            values of A (same sparsity pattern) on the device:
                            the CSR-entry -> element-slot maps of both device
@@ -439,7 +441,7 @@ typedef struct {
 /* Defaults: FP32 inner with FP64 reliable updates, tol 1e-10, max_iters
  * 100000, max_refinements 500, check_every 16, use_graph 1,
  * replace_ratio_f32 1e-2, replace_ratio_f64 1e-4, variant AUTO, prec GIVEN,
- * factor_bf16 0, reorder AUTO, matrix_f16 0, factor_f16 0, refresh 0. */
+ * factor_bf16 0, reorder AUTO, matrix_f16 0, factor_f16 1, refresh 0. */
 void ispm_solver_default_opts(ispm_solver_opts *opts);
 
 typedef struct ispm_solver ispm_solver;

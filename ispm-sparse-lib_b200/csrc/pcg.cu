@@ -1140,7 +1140,7 @@ void ispm_solver_default_opts(ispm_solver_opts *o)
   o->factor_bf16 = 0;
   o->reorder = ISPM_REORDER_AUTO;
   o->matrix_f16 = 0;
-  o->factor_f16 = 0;
+  o->factor_f16 = 1;
   o->refresh = 0;
 }
 

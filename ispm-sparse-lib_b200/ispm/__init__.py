@@ -778,7 +778,8 @@ class PCGSolver:
                  check_every: int = 16, use_graph: bool = True,
                  replace_ratio: float | None = None, variant: str = "auto",
                  prec: str = "given", factor_bf16: bool = False, reorder: str = "auto",
-                 matrix_f16: bool = False, factor_f16: bool = False, refresh: bool = False):
+                 matrix_f16: bool = False, factor_f16: bool | None = None,
+                 refresh: bool = False):
         _declare_solver()
         L = _lib()
         o = solver_opts()
@@ -793,7 +794,8 @@ class PCGSolver:
         o.factor_bf16 = int(factor_bf16)
         o.reorder = {"none": 0, "rcm": 1, "auto": 2}[reorder]
         o.matrix_f16 = int(matrix_f16)
-        o.factor_f16 = int(factor_f16)
+        if factor_f16 is not None:  # None: the library default (on)
+            o.factor_f16 = int(factor_f16)
         o.refresh = int(refresh)
         if A.elms.dtype != np.float64:
             raise TypeError("the solver takes the FP64 matrix")

@@ -78,7 +78,7 @@ def test_solver_default_options(ispm):
     assert (o.max_iters, o.max_refinements, o.check_every, o.use_graph) == (100000, 500, 16, 1)
     assert o.replace_ratio_f32 == 1e-2 and o.replace_ratio_f64 == 1e-4
     assert (o.variant, o.prec, o.factor_bf16, o.reorder) == (0, 0, 0, 2)
-    assert o.matrix_f16 == 0 and o.factor_f16 == 0
+    assert o.matrix_f16 == 0 and o.factor_f16 == 1 and o.refresh == 0
 
 
 def test_solver_rejects_malformed_csr_before_reordering(ispm, gen):
