@@ -469,7 +469,11 @@ __global__ void __launch_bounds__(1024, 2) slell_spmv_lanes_kernel(SpmvArgs<T, E
 template <class T, class E, int H, int W, bool VAR, bool DIAG, bool LANES = false>
 int launch_one(const SpmvArgs<T, E> &args, unsigned tps, cudaStream_t stream)
 {
-  const unsigned block = tps >= 256 ? tps : 256;
+  // A fused dot ends every CTA with a block reduction, a fence and an
+  // arrival on the counter: 1024-thread CTAs do that a quarter as often
+  // (the C2 mixed solve measured 58.2 against 59.5 ms, same iterations).
+  const unsigned block = (!LANES && args.ep.out) ? (tps >= 1024 ? tps : 1024)
+                                                 : (tps >= 256 ? tps : 256);
   const unsigned spb = block / tps;
   // lane-segmented: every virtual tile takes 1024 / (spb * S) CTAs
   const unsigned grid = LANES ? args.ln.n_vt * (1024u / (spb * args.slice_height))
