@@ -366,7 +366,13 @@ typedef struct {
   int max_iters;        /* total iterations */
   int max_refinements;  /* reliable updates + restarts */
   int check_every;      /* iterations per CUDA-graph chunk between host checks */
-  int use_graph;        /* replay iteration chunks as a CUDA graph */
+  int use_graph;        /* 1: replay iteration chunks as a CUDA graph, the host
+                           reading the device flags after each chunk; 2 (the
+                           classic iteration of an FP32 inner solve; others
+                           as 1): the chunk is the body of the graph's while
+                           node, repeated on the device until the flags end
+                           the phase, so a phase is one graph launch and one
+                           host wait; 0: eager launches */
   double replace_ratio_f32; /* reliable update once the recursive residual fell by
                                this factor since the last one (FP32 inner) */
   double replace_ratio_f64; /* same for FP64 */

@@ -361,19 +361,28 @@ __global__ void __launch_bounds__(kThreads)
 // ran).  With a preconditioner: every block first evaluates the stop test on
 // rr (from the G^T SpMV) and block 0 records it; the scalars roll in the
 // next update kernel, so no cross-block finish is needed here.
+// loop: launched inside the body of a graph's while node; block 0 ends the
+// loop (condition 0) once the solve needs the host.
 template <class T>
 __global__ void __launch_bounds__(kThreads)
     cg_direction_kernel(const T *__restrict__ z, T *__restrict__ p, long long n, PcgState *st,
-                        Scratch sc, int noprec)
+                        Scratch sc, int noprec, cudaGraphConditionalHandle loop, int in_loop)
 {
   pdl_wait();
-  if (st->done)
+  const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+  if (st->done) {
+    if (in_loop && lead)
+      cudaGraphSetConditional(loop, 0u);
     return;
+  }
   if (!noprec) {
     const double rr = st->rr;
     if (cg_stop(st, rr)) {
-      if (blockIdx.x == 0 && threadIdx.x == 0)
+      if (lead) {
         cg_flags(st, rr);
+        if (in_loop)
+          cudaGraphSetConditional(loop, 0u);
+      }
       return;
     }
   }
@@ -382,8 +391,11 @@ __global__ void __launch_bounds__(kThreads)
   const double beta = fresh ? 0.0 : rzn / st->rz;
   if (!(rzn > 0.0) || !isfinite(beta)) {
     // M is not positive definite on this residual (or r vanished exactly)
-    if (blockIdx.x == 0 && threadIdx.x == 0)
+    if (lead) {
       st->done = rzn == 0.0 ? kConverged : kBreakdown;
+      if (in_loop)
+        cudaGraphSetConditional(loop, 0u);
+    }
     return;
   }
   const T b = (T)beta;
@@ -579,6 +591,11 @@ struct Solver {
   void *vec[11] = {};
   enum { R, U, W, M, NV, P, S, Q, Z, D, TT };
   cudaGraphExec_t graph = nullptr;
+  // use_graph 2 (classic iteration): the chunk is the body of the graph's
+  // while node, whose condition the direction kernel clears; set while the
+  // body is being captured
+  cudaGraphConditionalHandle loop = 0;
+  bool capturing_loop = false;
   // The solve runs on the solver's own stream (the legacy default stream
   // cannot be captured into a graph), ordered after / before the caller's
   // stream with two events.
@@ -682,7 +699,8 @@ struct Solver {
     const T *z = (const T *)(have_prec ? vec[Z] : vec[R]);
     ISPM_CUDA_TRY(launch_kernel(cg_direction_kernel<T>, dim3(grid_for(n_pad)), dim3(kThreads), 0,
                                 s, true, z, (T *)vec[P], (long long)n_pad, st, sc,
-                                have_prec ? 0 : 1));
+                                have_prec ? 0 : 1, capturing_loop ? loop : 0ULL,
+                                capturing_loop ? 1 : 0));
     return launched("cg direction");
   }
 
@@ -718,16 +736,49 @@ struct Solver {
     return cg_direction<T>(s);
   }
 
+  // The chunk of check_every iterations as a graph; with use_graph 2 (classic
+  // iteration) the chunk is the body of a while node that repeats until the
+  // direction kernel clears the condition, so a phase is one graph launch
+  // and one host wait instead of one per chunk.
   int build_graph(cudaStream_t s)
   {
     if (graph)
       return ISPM_OK;
     cudaGraph_t g;
-    ISPM_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e;
     int err = ISPM_OK;
-    for (int k = 0; k < opts.check_every && !err; k++)
-      err = iteration(s);
-    cudaError_t e = cudaStreamEndCapture(s, &g);
+    if (opts.use_graph == 2 && classic) {
+      ISPM_CUDA_TRY(cudaGraphCreate(&g, 0));
+      e = cudaGraphConditionalHandleCreate(&loop, g, 1u, cudaGraphCondAssignDefault);
+      cudaGraphNodeParams np = {};
+      np.type = cudaGraphNodeTypeConditional;
+      np.conditional.handle = loop;
+      np.conditional.type = cudaGraphCondTypeWhile;
+      np.conditional.size = 1;
+      cudaGraphNode_t node;
+      if (e == cudaSuccess)
+        e = cudaGraphAddNode(&node, g, nullptr, 0, &np);
+      if (e == cudaSuccess)
+        e = cudaStreamBeginCaptureToGraph(s, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal);
+      if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return fail(ISPM_ERR_CUDA, "graph loop node: %s", cudaGetErrorString(e));
+      }
+      capturing_loop = true;
+      for (int k = 0; k < opts.check_every && !err; k++)
+        err = iteration(s);
+      capturing_loop = false;
+      cudaGraph_t body;
+      e = cudaStreamEndCapture(s, &body);
+      if (err || e != cudaSuccess)
+        cudaGraphDestroy(g);
+    } else {
+      ISPM_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      for (int k = 0; k < opts.check_every && !err; k++)
+        err = iteration(s);
+      e = cudaStreamEndCapture(s, &g);
+    }
     if (err)
       return err;
     if (e != cudaSuccess)

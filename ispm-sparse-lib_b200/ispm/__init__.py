@@ -770,12 +770,15 @@ class PCGSolver:
     fallen by replace_ratio since the previous one.  matrix_f16 (FP32 inner
     only): the inner iterations use the FP16 split of A (csr_split_f16).
     refresh: keep the maps update_values needs (new values of A, same
-    pattern, rewritten on the device)."""
+    pattern, rewritten on the device).  use_graph: True (1) replays chunks of
+    check_every iterations as a CUDA graph, 2 runs the chunk inside the
+    graph's while node until the device flags end the phase (classic
+    iteration), False launches eagerly."""
 
     def __init__(self, A: csr_matrix, G1: csr_matrix | None = None,
                  G2: csr_matrix | None = None, inner=np.float32, tol: float = 1e-10,
                  max_iters: int = 100000, max_refinements: int = 500,
-                 check_every: int = 16, use_graph: bool = True,
+                 check_every: int = 16, use_graph: bool | int = True,
                  replace_ratio: float | None = None, variant: str = "auto",
                  prec: str = "given", factor_bf16: bool = False, reorder: str = "auto",
                  matrix_f16: bool = False, factor_f16: bool | None = None,

@@ -71,7 +71,8 @@ def test_pcg_mixed_matches_fp64_iterations(ispm, oracle, cuda, gen):
 def test_pcg_device_vectors_graph_and_eager_agree(ispm, oracle, cuda, c1):
     A, b, G1, G2 = c1
     outs = []
-    for use_graph in (True, False):
+    # use_graph 2: the chunk repeats inside the graph's while node
+    for use_graph in (True, False, 2):
         s = ispm.PCGSolver(A, G1, G2, inner=np.float32, tol=1e-10, use_graph=use_graph)
         bd = cuda.zeros(s.rows, dtype=cuda.float64, device="cuda")
         bd[: A.n_rows] = cuda.from_numpy(b).cuda()
@@ -79,9 +80,35 @@ def test_pcg_device_vectors_graph_and_eager_agree(ispm, oracle, cuda, c1):
         st = s.solve(bd, xd)
         assert st["converged"]
         outs.append((xd.cpu().numpy(), st))
-    assert np.array_equal(outs[0][0], outs[1][0])
-    assert outs[0][1]["iterations"] == outs[1][1]["iterations"]
+    for k in (1, 2):
+        assert np.array_equal(outs[0][0], outs[k][0])
+        assert outs[0][1]["iterations"] == outs[k][1]["iterations"]
+        assert outs[0][1]["refinements"] == outs[k][1]["refinements"]
     assert true_relres(oracle, A, b, outs[0][0][: A.n_rows]) <= 1e-10
+
+
+def test_pcg_device_loop_stops(ispm, oracle, cuda, c1):
+    """The while-node loop ends on every flag the direction kernel or the
+    update raises: convergence without a preconditioner (the update's stop
+    test), the iteration cap, and a breakdown."""
+    A, b, G1, G2 = c1
+    for prec in ((G1, G2), (None, None)):
+        x, st = ispm.PCGSolver(A, *prec, inner=np.float32, tol=1e-9, use_graph=2,
+                               check_every=4).solve_host(b)
+        ref, st_ref = ispm.PCGSolver(A, *prec, inner=np.float32, tol=1e-9).solve_host(b)
+        assert st["converged"] and st["iterations"] == st_ref["iterations"]
+        assert np.array_equal(x, ref)
+    s = ispm.PCGSolver(A, G1, G2, inner=np.float32, tol=1e-14, max_iters=5, use_graph=2)
+    x, st = s.solve_host(b)
+    assert not st["converged"] and st["status"] == ispm.ERR_NOT_CONVERGED
+    assert st["iterations"] <= 5 + 16
+    n = 64
+    d = np.where(np.arange(n) % 2 == 0, 2.0, -2.0)
+    rp = np.arange(n + 1, dtype=np.int32)
+    Ai = ispm.csr_matrix(n, n, rp, np.arange(n, dtype=np.int32), d)
+    x, st = ispm.PCGSolver(Ai, None, None, inner=np.float32, tol=1e-10, max_refinements=5,
+                           use_graph=2).solve_host(np.ones(n))
+    assert st["status"] == ispm.ERR_BREAKDOWN and np.all(np.isfinite(x))
 
 
 def test_pcg_without_preconditioner_and_grf(ispm, oracle, cuda, gen):
