@@ -51,7 +51,11 @@ def test_pcg_with_gpu_fsai(ispm, oracle, cuda, gen):
     b = oracle.csr_spmv_f64(A.row_ptr, A.cols, A.elms, x_true)
     G1, G2 = ispm.fastainv_sym(A, np.float64, None, 200_000_000, 0.01)
     its = {}
+    # fsai_gpu32: the internal build with FP32 factor values, the operator the
+    # exported pair gives (the default stores an FP32 inner solve's factor
+    # as FP16 x 2^k, a slightly different preconditioner)
     for label, kw in (("ainv", dict(G1=G1, G2=G2)), ("fsai_gpu", dict(prec="fsai_gpu")),
+                      ("fsai_gpu32", dict(prec="fsai_gpu", factor_f16=False)),
                       ("fsai_pair", "pair")):
         if kw == "pair":
             F1, F2 = ispm.fsai_sym_gpu(A, np.float64)
@@ -66,7 +70,8 @@ def test_pcg_with_gpu_fsai(ispm, oracle, cuda, gen):
     # residual-equivalent: within 15% of the AINV iteration count
     for inner in (np.float64, np.float32):
         assert its[("fsai_gpu", inner)] <= 1.15 * its[("ainv", inner)], its
-        assert its[("fsai_gpu", inner)] == its[("fsai_pair", inner)]
+        assert its[("fsai_gpu32", inner)] == its[("fsai_pair", inner)], its
+        assert abs(its[("fsai_gpu", inner)] - its[("fsai_pair", inner)]) <= 3, its
 
 
 @pytest.mark.parametrize("prec", ["fsai_gpu", "ainv"])
