@@ -1085,12 +1085,17 @@ int build_fsai_on_device(Solver &S, int n, const int *rp, const int *ci, const d
                           &pos_t, false, bf16, f16))
     return e;
   if (f16) {
-    // FP16 factor values: eight rows a thread (one 16-byte element load per
-    // step); on the 128^3 27-point GRF system G and G^T took 24.6 against
-    // 25.8 us and the solve 57.5 against 58.3 ms, same results bit for bit
+    // FP16 factor values in diagonal blocks with at least eight stored
+    // entries a row: eight rows a thread (one 16-byte element load per
+    // step).  On the 128^3 27-point GRF system (14 a row) G and G^T took
+    // 24.6 against 25.8 us and the solve 57.5 against 58.3 ms, same results
+    // bit for bit; on the 192^3 unstructured system (4 a row) the solve took
+    // 19.5 against 18.3 ms, so short rows keep four
     for (Operator *o : {&S.G, &S.Ht}) {
       const ispm_slell_view m = o->dev.view();
-      if (m.hblock == 1 && !m.var_height && m.slice_height >= 32) {
+      const unsigned long long rows = (unsigned long long)m.n_slices * m.slice_height;
+      if (m.diags && m.hblock == 1 && !m.var_height && m.slice_height >= 32 &&
+          (unsigned long long)m.n_elms >= 8ull * rows) {
         o->lp.H = 8;
         o->lp.N = m.slice_height / 8;
       }
